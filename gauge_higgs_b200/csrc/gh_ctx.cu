@@ -1,0 +1,817 @@
+// gh_ctx.cu -- context, device memory, trajectory graph and the C ABI of
+// include/gauge_higgs_b200.h.
+#include <cuda_runtime.h>
+#include <algorithm>
+#include <cstddef>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <string>
+#include <vector>
+#include "gh_engine.cuh"
+#include "../../include/gauge_higgs_b200.h"
+
+using namespace ghk;
+
+namespace {
+thread_local std::string g_err;
+}
+
+struct gh_ctx {
+  int D = 0, N = 0, ng = 0, nlat = 0, prec = 0, rep = 0, d = 0, real = 0, scalar = 0;
+  size_t rs = 8;                      // bytes per real of the field storage
+  std::vector<LatDev> lat_h;          // host copy (extents, offsets; counters live on the device)
+  long long nU = 0, nP = 0, nF = 0, nG = 0;   // total complex / real / complex / complex elements
+  Bufs b{};
+  std::unique_ptr<EngineBase> eng;
+  cudaStream_t own = nullptr, st = nullptr;
+  int integ = 1, nmd = 20;
+  double tau = 1.0;
+  cudaGraphExec_t gexec = nullptr;
+  cudaGraph_t graph = nullptr;
+  int use_graph = 1;
+  double* staging = nullptr;
+  size_t staging_elems = 0;
+  double* fbuf = nullptr;             // FP64 SoA force output (links)
+  double* fphibuf = nullptr;          // FP64 SoA force output (vectors)
+  std::vector<void*> allocs;
+  std::string err;
+  uint64_t bytes = 0;
+  // tempering
+  int temper = 0;
+  uint64_t swap_seed = 0;
+  int* t_order = nullptr;             // [nlat] lattice currently holding the k-th kappa (grouped)
+  int* t_groups = nullptr;            // [ngroups+1] group boundaries into t_order
+  int t_ngroups = 0;
+  unsigned long long* t_stats = nullptr;   // [2*nlat + 1] attempts, accepts, counter
+  int* t_pairmap = nullptr;
+  ~gh_ctx() {
+    if (st) cudaStreamSynchronize(st);
+    if (gexec) cudaGraphExecDestroy(gexec);
+    if (graph) cudaGraphDestroy(graph);
+    for (void* p : allocs) cudaFree(p);
+    if (own) cudaStreamDestroy(own);
+  }
+};
+
+namespace {
+
+int fail(gh_ctx* c, int code, const std::string& m) {
+  if (c) c->err = m; else g_err = m;
+  return code;
+}
+#define CK(call)                                                                          \
+  do {                                                                                    \
+    cudaError_t e_ = (call);                                                              \
+    if (e_ != cudaSuccess)                                                                \
+      return fail(ctx, GH_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+  } while (0)
+
+template <typename T>
+int dalloc(gh_ctx* ctx, T** p, size_t n) {
+  void* q = nullptr;
+  const size_t bytes = std::max<size_t>(n, 1) * sizeof(T);
+  cudaError_t e = cudaMalloc(&q, bytes);
+  if (e != cudaSuccess) return fail(ctx, GH_ERR_CUDA, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+  cudaMemset(q, 0, bytes);
+  ctx->allocs.push_back(q);
+  ctx->bytes += bytes;
+  *p = (T*)q;
+  return GH_OK;
+}
+
+int launch_check(gh_ctx* ctx, const char* what) {
+  cudaError_t e = cudaPeekAtLastError();
+  if (e != cudaSuccess) { cudaGetLastError(); return fail(ctx, GH_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e)); }
+  return GH_OK;
+}
+
+void invalidate_graph(gh_ctx* ctx) {
+  if (ctx->gexec) { cudaGraphExecDestroy(ctx->gexec); ctx->gexec = nullptr; }
+  if (ctx->graph) { cudaGraphDestroy(ctx->graph); ctx->graph = nullptr; }
+}
+
+// ---- integrator building blocks (enqueue only) ----
+void enq_kick(gh_ctx* ctx, double eps) {
+  if (ctx->rep == REP_GEN) ctx->eng->gen_links(ctx->b, eps, 0, nullptr);
+  ctx->eng->kick(ctx->b, eps, M_UPDATE, F_GAUGE | F_MATTER, nullptr, true, true);
+}
+void enq_drift(gh_ctx* ctx, double eps) { ctx->eng->drift(ctx->b, eps, ctx->prec == GH_PREC_FP32_MD ? 1 : 0); }
+
+// md_evolve: src/hmc/gauge_higgs_hmc.hpp:149-165 (identical in src/hmc/hmc.hpp:54-70)
+void enq_md(gh_ctx* ctx) {
+  const double eps = ctx->tau / ctx->nmd;
+  if (ctx->integ == GH_LEAPFROG) {
+    enq_kick(ctx, 0.5 * eps);
+    for (int i = 0; i < ctx->nmd; ++i) { enq_drift(ctx, eps); if (i != ctx->nmd - 1) enq_kick(ctx, eps); }
+    enq_kick(ctx, 0.5 * eps);
+  } else {
+    const double lam = 0.1931833275037836;   // src/core/config.hpp:25
+    enq_kick(ctx, lam * eps);
+    for (int i = 0; i < ctx->nmd; ++i) {
+      enq_drift(ctx, 0.5 * eps);
+      enq_kick(ctx, (1.0 - 2.0 * lam) * eps);
+      enq_drift(ctx, 0.5 * eps);
+      enq_kick(ctx, (i != ctx->nmd - 1 ? 2.0 * lam : lam) * eps);
+    }
+  }
+}
+
+void enq_measure(gh_ctx* ctx, int slot) {
+  ctx->eng->measure(ctx->b);
+  FinArgs f;
+  f.lats = ctx->b.lats; f.blk_first = ctx->b.blk_first; f.partials = ctx->b.partials; f.res = ctx->b.res;
+  f.slot = slot; f.D = ctx->D; f.N = ctx->N; f.scalar = ctx->scalar;
+  k_finalize<<<ctx->nlat, 32, 0, ctx->st>>>(f);
+}
+
+// Replica-tempering pass in kappa (src/hmc/replica_tempering.hpp:157-205 mechanism).
+struct TemperArgs {
+  LatDev* lats; const double* res; int* order; const int* groups; int ngroups; int D;
+  unsigned long long* stats; const int* pairmap; int nlat; unsigned long long seed;
+};
+__global__ void k_temper(const TemperArgs a) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  unsigned long long& counter = a.stats[2 * a.nlat];
+  for (int g = 0; g < a.ngroups; ++g) {
+    const int b0 = a.groups[g], b1 = a.groups[g + 1];
+    for (int start = 0; start < 2; ++start)
+      for (int k = b0 + start; k + 1 < b1; k += 2) {
+        const int li = a.order[k], lj = a.order[k + 1];
+        LatDev& Li = a.lats[li];
+        LatDev& Lj = a.lats[lj];
+        const double* ri = a.res + ((size_t)li * 2 + (Li.last_acc ? 1 : 0)) * NRES;
+        const double* rj = a.res + ((size_t)lj * 2 + (Lj.last_acc ? 1 : 0)) * NRES;
+        const double Bi = 2.0 * ri[6] * (double)Li.V * a.D;
+        const double Bj = 2.0 * rj[6] * (double)Lj.V * a.D;
+        const double delta = (Li.kappa - Lj.kappa) * (Bi - Bj);
+        const int pid = a.pairmap[k];
+        a.stats[pid] += 1;
+        bool acc = (delta <= 0.0);
+        counter += 1;
+        if (!acc) acc = ghrng::uniform(a.seed, ghrng::key(0x57A9, counter)) < exp(-delta);
+        if (acc) {
+          const double tk = Li.kappa; Li.kappa = Lj.kappa; Lj.kappa = tk;
+          const int tc = Li.cidx; Li.cidx = Lj.cidx; Lj.cidx = tc;
+          a.order[k] = lj; a.order[k + 1] = li;
+          a.stats[a.nlat + pid] += 1;
+        }
+      }
+  }
+}
+
+void enq_trajectory(gh_ctx* ctx) {
+  Bufs& b = ctx->b;
+  InitArgs ia{};
+  ia.what = 1; ia.pure = ctx->scalar ? 0 : 1; ia.real = ctx->real; ia.d = ctx->d; ia.vec = b.pi;
+  ctx->eng->init(b, ia, true, ctx->scalar != 0);
+  cudaMemcpyAsync(b.Us, b.U, (size_t)ctx->nU * 2 * ctx->rs, cudaMemcpyDeviceToDevice, ctx->st);
+  if (ctx->scalar) cudaMemcpyAsync(b.phis, b.phi, (size_t)ctx->nF * 2 * ctx->rs, cudaMemcpyDeviceToDevice, ctx->st);
+  enq_measure(ctx, 0);
+  enq_md(ctx);
+  if (ctx->prec == GH_PREC_FP64) ctx->eng->reunit(b);
+  enq_measure(ctx, 1);
+  MetroArgs m;
+  m.lats = b.lats; m.res = b.res; m.hist = b.hist; m.hist_cap = b.hist_cap; m.nlat = ctx->nlat; m.pure = ctx->scalar ? 0 : 1;
+  k_metropolis<<<(ctx->nlat + 63) / 64, 64, 0, ctx->st>>>(m);
+  ctx->eng->restore(b);
+  if (ctx->temper && ctx->scalar) {
+    TemperArgs t;
+    t.lats = b.lats; t.res = b.res; t.order = ctx->t_order; t.groups = ctx->t_groups; t.ngroups = ctx->t_ngroups;
+    t.D = ctx->D; t.stats = ctx->t_stats; t.pairmap = ctx->t_pairmap; t.nlat = ctx->nlat; t.seed = ctx->swap_seed;
+    k_temper<<<1, 32, 0, ctx->st>>>(t);
+  }
+}
+
+int run_traj(gh_ctx* ctx) {
+  if (ctx->use_graph) {
+    if (!ctx->gexec) {
+      CK(cudaStreamBeginCapture(ctx->st, cudaStreamCaptureModeThreadLocal));
+      enq_trajectory(ctx);
+      cudaGraph_t g = nullptr;
+      cudaError_t e = cudaStreamEndCapture(ctx->st, &g);
+      if (e != cudaSuccess) { cudaGetLastError(); return fail(ctx, GH_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(e)); }
+      ctx->graph = g;
+      CK(cudaGraphInstantiate(&ctx->gexec, g, 0));
+    }
+    CK(cudaGraphLaunch(ctx->gexec, ctx->st));
+  } else {
+    enq_trajectory(ctx);
+  }
+  return launch_check(ctx, "trajectory");
+}
+
+int check_lat(gh_ctx* ctx, int lat, bool allow_all) {
+  if (!ctx) return fail(nullptr, GH_ERR_ARG, "null context");
+  if (lat == -1 && allow_all) return GH_OK;
+  if (lat < 0 || lat >= ctx->nlat) return fail(ctx, GH_ERR_ARG, "lattice index out of range");
+  return GH_OK;
+}
+
+// AoS host <-> SoA device for one lattice. kind 0 links, 1 momenta, 2 vectors.
+int xfer_one(gh_ctx* ctx, int lat, int kind, void* dev, double* host, bool to_dev, bool dev_is_fp64 = false) {
+  const LatDev& L = ctx->lat_h[lat];
+  const int ncomp = kind == 0 ? ctx->N * ctx->N : kind == 1 ? ctx->ng : ctx->d;
+  const size_t nd = (size_t)L.V * (kind == 2 ? ncomp : ctx->D * ncomp) * (kind == 1 ? 1 : 2);
+  if (to_dev) CK(cudaMemcpyAsync(ctx->staging, host, nd * sizeof(double), cudaMemcpyHostToDevice, ctx->st));
+  XferArgs a;
+  a.lat = lat; a.kind = kind; a.D = ctx->D; a.ncomp = ncomp; a.host_aos = ctx->staging; a.dev = dev; a.to_dev = to_dev ? 1 : 0;
+  if (dev_is_fp64) {
+    a.lats = ctx->b.lats;
+    k_xfer<double><<<296, 256, 0, ctx->st>>>(a);
+  } else {
+    ctx->eng->xfer(ctx->b, a);
+  }
+  int rc = launch_check(ctx, "xfer");
+  if (rc) return rc;
+  if (!to_dev) {
+    CK(cudaMemcpyAsync(host, ctx->staging, nd * sizeof(double), cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
+  }
+  return GH_OK;
+}
+
+size_t lat_elems(const gh_ctx* ctx, int lat, int kind) {
+  const LatDev& L = ctx->lat_h[lat];
+  return (size_t)L.V * (kind == 0 ? ctx->D * ctx->N * ctx->N * 2 : kind == 1 ? ctx->D * ctx->ng : ctx->d * 2);
+}
+
+int xfer_field(gh_ctx* ctx, int lat, int kind, void* dev, const double* host, bool to_dev) {
+  int rc = check_lat(ctx, lat, true);
+  if (rc) return rc;
+  if (kind == 2 && !ctx->scalar) return fail(ctx, GH_ERR_STATE, "no scalar field in a pure-gauge context");
+  if (!host) return fail(ctx, GH_ERR_ARG, "null host pointer");
+  const int l0 = lat < 0 ? 0 : lat, l1 = lat < 0 ? ctx->nlat : lat + 1;
+  size_t off = 0;
+  for (int l = l0; l < l1; ++l) {
+    rc = xfer_one(ctx, l, kind, dev, const_cast<double*>(host) + off, to_dev);
+    if (rc) return rc;
+    if (to_dev) { CK(cudaStreamSynchronize(ctx->st)); }
+    off += lat_elems(ctx, l, kind);
+  }
+  return GH_OK;
+}
+
+int build_general(gh_ctx* ctx, const gh_rep_desc* r) {
+  const int d = r->d, N = ctx->N, ng = ctx->ng;
+  const long dimT = r->dimT;
+  if (d <= 0 || r->n_boxes <= 0 || r->n_boxes > 15 || dimT <= 0 || !r->T || !r->W)
+    return fail(ctx, GH_ERR_REP, "general representation needs d, n_boxes, dimT, T and W");
+  long pw = 1;
+  for (int k = 0; k < r->n_boxes; ++k) pw *= N;
+  if (pw != dimT) return fail(ctx, GH_ERR_REP, "dimT must equal N^n_boxes");
+  if (dimT > 200000) return fail(ctx, GH_ERR_REP, "N^n exceeds the 200000 cap of the reference (src/rep/rep_general.hpp:34)");
+  const double* W = r->W;
+  const double* T = r->T;
+  std::vector<int> wt_ptr(dimT + 1, 0), wt_l, w_ptr(d + 1, 0), w_i, t_ptr(ng * d + 1, 0), t_j;
+  std::vector<double2> wt_v, w_v, t_v;
+  for (long i = 0; i < dimT; ++i) {
+    for (int l = 0; l < d; ++l) {
+      const double re = W[2 * ((size_t)l * dimT + i)], im = W[2 * ((size_t)l * dimT + i) + 1];
+      if (re != 0.0 || im != 0.0) { wt_l.push_back(l); wt_v.push_back(make_double2(re, im)); }
+    }
+    wt_ptr[i + 1] = (int)wt_l.size();
+  }
+  for (int l = 0; l < d; ++l) {
+    for (long i = 0; i < dimT; ++i) {
+      const double re = W[2 * ((size_t)l * dimT + i)], im = W[2 * ((size_t)l * dimT + i) + 1];
+      if (re != 0.0 || im != 0.0) { w_i.push_back((int)i); w_v.push_back(make_double2(re, im)); }
+    }
+    w_ptr[l + 1] = (int)w_i.size();
+  }
+  for (int a = 0; a < ng; ++a)
+    for (int i = 0; i < d; ++i) {
+      for (int j = 0; j < d; ++j) {
+        const size_t o = 2 * (((size_t)a * d + i) * d + j);
+        if (T[o] != 0.0 || T[o + 1] != 0.0) { t_j.push_back(j); t_v.push_back(make_double2(T[o], T[o + 1])); }
+      }
+      t_ptr[a * d + i + 1] = (int)t_j.size();
+    }
+  GenTables& t = ctx->b.gen;
+  t.d = d; t.n = r->n_boxes; t.dimT = (int)dimT; t.ng = ng;
+  t.powN[0] = 1;
+  for (int k = 1; k < 16; ++k) t.powN[k] = (k <= r->n_boxes) ? t.powN[k - 1] * N : 0;
+  int *p1, *p2, *p3, *p4, *p5, *p6;
+  double2 *v1, *v2, *v3;
+  int rc;
+  if ((rc = dalloc(ctx, &p1, wt_ptr.size())) || (rc = dalloc(ctx, &p2, wt_l.size())) || (rc = dalloc(ctx, &v1, wt_v.size())) ||
+      (rc = dalloc(ctx, &p3, w_ptr.size())) || (rc = dalloc(ctx, &p4, w_i.size())) || (rc = dalloc(ctx, &v2, w_v.size())) ||
+      (rc = dalloc(ctx, &p5, t_ptr.size())) || (rc = dalloc(ctx, &p6, t_j.size())) || (rc = dalloc(ctx, &v3, t_v.size())))
+    return rc;
+  CK(cudaMemcpy(p1, wt_ptr.data(), wt_ptr.size() * 4, cudaMemcpyHostToDevice));
+  if (!wt_l.empty()) CK(cudaMemcpy(p2, wt_l.data(), wt_l.size() * 4, cudaMemcpyHostToDevice));
+  if (!wt_v.empty()) CK(cudaMemcpy(v1, wt_v.data(), wt_v.size() * 16, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(p3, w_ptr.data(), w_ptr.size() * 4, cudaMemcpyHostToDevice));
+  if (!w_i.empty()) CK(cudaMemcpy(p4, w_i.data(), w_i.size() * 4, cudaMemcpyHostToDevice));
+  if (!w_v.empty()) CK(cudaMemcpy(v2, w_v.data(), w_v.size() * 16, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(p5, t_ptr.data(), t_ptr.size() * 4, cudaMemcpyHostToDevice));
+  if (!t_j.empty()) CK(cudaMemcpy(p6, t_j.data(), t_j.size() * 4, cudaMemcpyHostToDevice));
+  if (!t_v.empty()) CK(cudaMemcpy(v3, t_v.data(), t_v.size() * 16, cudaMemcpyHostToDevice));
+  t.wt_ptr = p1; t.wt_l = p2; t.wt_v = v1; t.w_ptr = p3; t.w_i = p4; t.w_v = v2; t.t_ptr = p5; t.t_j = p6; t.t_v = v3;
+  return GH_OK;
+}
+
+}  // namespace
+
+// ===========================================================================
+// C ABI
+// ===========================================================================
+extern "C" {
+
+const char* gh_last_error(const gh_ctx* ctx) { return ctx ? ctx->err.c_str() : g_err.c_str(); }
+
+int gh_ctx_create(int D, int N, int n_lat, const int* L, const gh_rep_desc* rep, int precision,
+                  const uint64_t* seeds, gh_ctx** out) {
+  gh_ctx* ctx = nullptr;
+  if (!out) return fail(nullptr, GH_ERR_ARG, "null output pointer");
+  *out = nullptr;
+  if (D < 2 || D > 4) return fail(nullptr, GH_ERR_UNSUPPORTED, "D must be 2, 3 or 4");
+  if (N < 2 || N > 3) return fail(nullptr, GH_ERR_UNSUPPORTED, "N must be 2 or 3");
+  if (n_lat < 1 || !L || !seeds) return fail(nullptr, GH_ERR_ARG, "need n_lat >= 1, extents and seeds");
+  if (precision != GH_PREC_FP64 && precision != GH_PREC_FP32_MD) return fail(nullptr, GH_ERR_ARG, "unknown precision");
+  int dev_count = 0;
+  if (cudaGetDeviceCount(&dev_count) != cudaSuccess || dev_count == 0) {
+    cudaGetLastError();
+    return fail(nullptr, GH_ERR_CUDA, "no CUDA device: the gauge_higgs_b200 engine has no CPU path");
+  }
+  std::unique_ptr<gh_ctx> c(new gh_ctx());
+  ctx = c.get();
+  ctx->D = D; ctx->N = N; ctx->ng = N * N - 1; ctx->nlat = n_lat; ctx->prec = precision;
+  ctx->rs = precision == GH_PREC_FP64 ? sizeof(double) : sizeof(float);
+  const int kind = rep ? rep->kind : GH_REP_NONE;
+  switch (kind) {
+    case GH_REP_NONE: ctx->rep = REP_NONE; ctx->d = 0; break;
+    case GH_REP_FUND: ctx->rep = REP_FUND; ctx->d = N; ctx->real = 0; break;
+    case GH_REP_ADJ: ctx->rep = REP_ADJ; ctx->d = N * N - 1; ctx->real = 1; break;
+    case GH_REP_GENERAL: ctx->rep = REP_GEN; ctx->d = rep->d; ctx->real = rep->real ? 1 : 0; break;
+    default: return fail(nullptr, GH_ERR_REP, "unknown representation kind");
+  }
+  if (kind == GH_REP_FUND && rep->d && rep->d != N) return fail(nullptr, GH_ERR_REP, "fundamental rep must have d = N");
+  if (kind == GH_REP_ADJ && rep->d && rep->d != N * N - 1) return fail(nullptr, GH_ERR_REP, "adjoint rep must have d = N^2-1");
+  ctx->scalar = ctx->rep != REP_NONE;
+  // lattices, offsets and work tables
+  long long u = 0, p = 0, f = 0, g = 0;
+  std::vector<Work> wl, ws;
+  std::vector<int> blk_first(1, 0);
+  size_t stage = 1;
+  for (int l = 0; l < n_lat; ++l) {
+    LatDev Ld{};
+    long long V = 1;
+    for (int mu = 0; mu < 4; ++mu) { Ld.L[mu] = 1; Ld.stride[mu] = 0; }
+    for (int mu = 0; mu < D; ++mu) {
+      if (L[l * D + mu] < 1) return fail(nullptr, GH_ERR_ARG, "lattice extents must be >= 1");
+      Ld.L[mu] = L[l * D + mu]; Ld.stride[mu] = (int)V; V *= L[l * D + mu];
+    }
+    if (V * D * N * N > (1LL << 31) - 1) return fail(nullptr, GH_ERR_ARG, "lattice too large for 32-bit site indexing");
+    Ld.V = (int)V; Ld.cidx = l;
+    Ld.u_off = u; Ld.p_off = p; Ld.f_off = f; Ld.g_off = g;
+    Ld.beta = 2.3; Ld.kappa = 0.1; Ld.lambda = 0.5; Ld.seed = seeds[l];
+    u += V * D * N * N; p += V * D * ctx->ng; f += V * ctx->d; g += (ctx->rep == REP_GEN) ? V * D * ctx->d : 0;
+    ctx->lat_h.push_back(Ld);
+    for (int mu = 0; mu < D; ++mu)
+      for (int s0 = 0; s0 < V; s0 += KBLOCK) wl.push_back(Work{l, mu, s0, (int)std::min<long long>(KBLOCK, V - s0)});
+    for (int s0 = 0; s0 < V; s0 += KBLOCK) ws.push_back(Work{l, -1, s0, (int)std::min<long long>(KBLOCK, V - s0)});
+    blk_first.push_back((int)ws.size());
+    stage = std::max<size_t>(stage, (size_t)V * std::max<size_t>(std::max<size_t>((size_t)D * N * N * 2, (size_t)D * ctx->ng), (size_t)ctx->d * 2));
+  }
+  ctx->nU = u; ctx->nP = p; ctx->nF = f; ctx->nG = g;
+  std::vector<Work> wg;
+  if (ctx->rep == REP_GEN)
+    for (int l = 0; l < n_lat; ++l)
+      for (int mu = 0; mu < D; ++mu)
+        for (int s0 = 0; s0 < ctx->lat_h[l].V; s0 += GEN_WARPS)
+          wg.push_back(Work{l, mu, s0, std::min(GEN_WARPS, ctx->lat_h[l].V - s0)});
+  std::vector<Work> wall = wl;
+  wall.insert(wall.end(), ws.begin(), ws.end());
+
+  ctx->eng.reset(N == 2 ? (precision == GH_PREC_FP64 ? make_engine_n2_f64(D, ctx->rep) : make_engine_n2_f32(D, ctx->rep))
+                        : (precision == GH_PREC_FP64 ? make_engine_n3_f64(D, ctx->rep) : make_engine_n3_f32(D, ctx->rep)));
+  if (!ctx->eng) return fail(nullptr, GH_ERR_UNSUPPORTED, "no kernel instance for this configuration");
+  CK(cudaStreamCreateWithFlags(&ctx->own, cudaStreamNonBlocking));
+  ctx->st = ctx->own;
+  Bufs& b = ctx->b;
+  const size_t rs = ctx->rs;
+  int rc;
+  unsigned char *U, *Us, *P, *phi = nullptr, *phis = nullptr, *pi = nullptr, *psif = nullptr, *psib = nullptr;
+  if ((rc = dalloc(ctx, &U, (size_t)u * 2 * rs)) || (rc = dalloc(ctx, &Us, (size_t)u * 2 * rs)) ||
+      (rc = dalloc(ctx, &P, (size_t)p * rs)))
+    { g_err = ctx->err; return rc; }
+  if (ctx->scalar) {
+    if ((rc = dalloc(ctx, &phi, (size_t)f * 2 * rs)) || (rc = dalloc(ctx, &phis, (size_t)f * 2 * rs)) ||
+        (rc = dalloc(ctx, &pi, (size_t)f * 2 * rs)))
+      { g_err = ctx->err; return rc; }
+  }
+  if (ctx->rep == REP_GEN) {
+    if ((rc = dalloc(ctx, &psif, (size_t)g * 2 * rs)) || (rc = dalloc(ctx, &psib, (size_t)g * 2 * rs))) { g_err = ctx->err; return rc; }
+    if ((rc = build_general(ctx, rep))) { g_err = ctx->err; return rc; }
+  }
+  b.U = U; b.Us = Us; b.P = P; b.phi = phi; b.phis = phis; b.pi = pi; b.psif = psif; b.psib = psib;
+  b.nw_links = (int)wl.size(); b.nw_sites = (int)ws.size(); b.nw_gen = (int)wg.size();
+  b.hist_cap = 1024;
+  b.nlat = n_lat; b.D = D; b.N = N; b.d = ctx->d; b.rep = ctx->rep; b.scalar = ctx->scalar; b.st = ctx->st;
+  if ((rc = dalloc(ctx, &b.lats, n_lat)) || (rc = dalloc(ctx, &b.w_all, wall.size())) ||
+      (rc = dalloc(ctx, &b.w_gen, std::max<size_t>(wg.size(), 1))) || (rc = dalloc(ctx, &b.blk_first, blk_first.size())) ||
+      (rc = dalloc(ctx, &b.partials, (size_t)ws.size() * NRED)) || (rc = dalloc(ctx, &b.res, (size_t)n_lat * 2 * NRES)) ||
+      (rc = dalloc(ctx, &b.hist, (size_t)n_lat * b.hist_cap)) || (rc = dalloc(ctx, &ctx->staging, stage)) ||
+      (rc = dalloc(ctx, &ctx->fbuf, (size_t)std::max<long long>(p, 1))) ||
+      (rc = dalloc(ctx, &ctx->fphibuf, (size_t)std::max<long long>(f, 1) * 2)))
+    { g_err = ctx->err; return rc; }
+  ctx->staging_elems = stage;
+  CK(cudaMemcpy(b.lats, ctx->lat_h.data(), sizeof(LatDev) * n_lat, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(b.w_all, wall.data(), sizeof(Work) * wall.size(), cudaMemcpyHostToDevice));
+  if (!wg.empty()) CK(cudaMemcpy(b.w_gen, wg.data(), sizeof(Work) * wg.size(), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(b.blk_first, blk_first.data(), sizeof(int) * blk_first.size(), cudaMemcpyHostToDevice));
+  if (ctx->rep == REP_GEN) {
+    const size_t sm = ctx->eng->gen_smem(b);
+    if (sm > 227 * 1024) { g_err = "general irrep too large for the shared-memory tensor buffer"; return GH_ERR_REP; }
+    if ((rc = ctx->eng->prepare(b))) { g_err = "cudaFuncSetAttribute failed for the general-irrep kernel"; return GH_ERR_CUDA; }
+  }
+  // identity links and zero fields as the starting state (GaugeField default is zero
+  // matrices; a cold start is the useful default for a device engine)
+  InitArgs ia{};
+  ia.what = 4;
+  ctx->eng->init(b, ia, true, false);
+  CK(cudaStreamSynchronize(ctx->st));
+  if ((rc = launch_check(ctx, "init"))) { g_err = ctx->err; return rc; }
+  *out = c.release();
+  return GH_OK;
+}
+
+int gh_ctx_destroy(gh_ctx* ctx) {
+  delete ctx;
+  return GH_OK;
+}
+
+int gh_set_stream(gh_ctx* ctx, void* stream) {
+  if (!ctx) return fail(nullptr, GH_ERR_ARG, "null context");
+  CK(cudaStreamSynchronize(ctx->st));
+  ctx->st = stream ? (cudaStream_t)stream : ctx->own;
+  ctx->b.st = ctx->st;
+  invalidate_graph(ctx);
+  return GH_OK;
+}
+
+int gh_sync(gh_ctx* ctx) {
+  if (!ctx) return fail(nullptr, GH_ERR_ARG, "null context");
+  CK(cudaStreamSynchronize(ctx->st));
+  return launch_check(ctx, "sync");
+}
+
+int gh_info(const gh_ctx* ctx, int* D, int* N, int* n_lat, int* d, int* rep_kind, int* precision) {
+  if (!ctx) return fail(nullptr, GH_ERR_ARG, "null context");
+  if (D) *D = ctx->D;
+  if (N) *N = ctx->N;
+  if (n_lat) *n_lat = ctx->nlat;
+  if (d) *d = ctx->d;
+  if (rep_kind) *rep_kind = ctx->rep;
+  if (precision) *precision = ctx->prec;
+  return GH_OK;
+}
+
+int gh_device_bytes(const gh_ctx* ctx, uint64_t* bytes) {
+  if (!ctx || !bytes) return fail(nullptr, GH_ERR_ARG, "null argument");
+  *bytes = ctx->bytes;
+  return GH_OK;
+}
+
+int gh_set_couplings(gh_ctx* ctx, int lat, double beta, double kappa, double lambda) {
+  int rc = check_lat(ctx, lat, true);
+  if (rc) return rc;
+  CK(cudaStreamSynchronize(ctx->st));
+  const int l0 = lat < 0 ? 0 : lat, l1 = lat < 0 ? ctx->nlat : lat + 1;
+  for (int l = l0; l < l1; ++l) {
+    double v[3] = {beta, kappa, lambda};
+    ctx->lat_h[l].beta = beta; ctx->lat_h[l].kappa = kappa; ctx->lat_h[l].lambda = lambda;
+    CK(cudaMemcpy((char*)(ctx->b.lats + l) + offsetof(LatDev, beta), v, sizeof(v), cudaMemcpyHostToDevice));
+  }
+  return GH_OK;
+}
+
+int gh_get_couplings(gh_ctx* ctx, int lat, double* beta, double* kappa, double* lambda) {
+  int rc = check_lat(ctx, lat, false);
+  if (rc) return rc;
+  LatDev L;
+  CK(cudaStreamSynchronize(ctx->st));
+  CK(cudaMemcpy(&L, ctx->b.lats + lat, sizeof(L), cudaMemcpyDeviceToHost));
+  if (beta) *beta = L.beta;
+  if (kappa) *kappa = L.kappa;
+  if (lambda) *lambda = L.lambda;
+  return GH_OK;
+}
+
+int gh_set_integrator(gh_ctx* ctx, int integ, int nmd, double tau) {
+  if (!ctx) return fail(nullptr, GH_ERR_ARG, "null context");
+  if ((integ != GH_LEAPFROG && integ != GH_OMELYAN) || nmd < 1 || !(tau > 0.0))
+    return fail(ctx, GH_ERR_ARG, "integrator must be leapfrog/omelyan with nmd >= 1 and tau > 0");
+  ctx->integ = integ; ctx->nmd = nmd; ctx->tau = tau;
+  invalidate_graph(ctx);
+  return GH_OK;
+}
+
+int gh_set_traj_count(gh_ctx* ctx, int lat, uint64_t traj_count, uint64_t accept_count) {
+  int rc = check_lat(ctx, lat, true);
+  if (rc) return rc;
+  CK(cudaStreamSynchronize(ctx->st));
+  const int l0 = lat < 0 ? 0 : lat, l1 = lat < 0 ? ctx->nlat : lat + 1;
+  for (int l = l0; l < l1; ++l) {
+    unsigned long long v[2] = {traj_count, accept_count};
+    CK(cudaMemcpy((char*)(ctx->b.lats + l) + offsetof(LatDev, traj), v, sizeof(v), cudaMemcpyHostToDevice));
+  }
+  return GH_OK;
+}
+
+int gh_get_traj_count(gh_ctx* ctx, int lat, uint64_t* traj_count, uint64_t* accept_count, uint64_t* nonfinite_count) {
+  int rc = check_lat(ctx, lat, false);
+  if (rc) return rc;
+  LatDev L;
+  CK(cudaStreamSynchronize(ctx->st));
+  CK(cudaMemcpy(&L, ctx->b.lats + lat, sizeof(L), cudaMemcpyDeviceToHost));
+  if (traj_count) *traj_count = L.traj;
+  if (accept_count) *accept_count = L.accepted;
+  if (nonfinite_count) *nonfinite_count = L.nonfinite;
+  return GH_OK;
+}
+
+int gh_set_links(gh_ctx* ctx, int lat, const double* U) { return xfer_field(ctx, lat, 0, ctx ? ctx->b.U : nullptr, U, true); }
+int gh_get_links(gh_ctx* ctx, int lat, double* U) { return xfer_field(ctx, lat, 0, ctx ? ctx->b.U : nullptr, U, false); }
+int gh_set_mom(gh_ctx* ctx, int lat, const double* P) { return xfer_field(ctx, lat, 1, ctx ? ctx->b.P : nullptr, P, true); }
+int gh_get_mom(gh_ctx* ctx, int lat, double* P) { return xfer_field(ctx, lat, 1, ctx ? ctx->b.P : nullptr, P, false); }
+int gh_set_phi(gh_ctx* ctx, int lat, const double* phi) { return xfer_field(ctx, lat, 2, ctx ? ctx->b.phi : nullptr, phi, true); }
+int gh_get_phi(gh_ctx* ctx, int lat, double* phi) { return xfer_field(ctx, lat, 2, ctx ? ctx->b.phi : nullptr, phi, false); }
+int gh_set_pi(gh_ctx* ctx, int lat, const double* pi) { return xfer_field(ctx, lat, 2, ctx ? ctx->b.pi : nullptr, pi, true); }
+int gh_get_pi(gh_ctx* ctx, int lat, double* pi) { return xfer_field(ctx, lat, 2, ctx ? ctx->b.pi : nullptr, pi, false); }
+
+int gh_hot_start(gh_ctx* ctx, double sigma) {
+  if (!ctx) return fail(nullptr, GH_ERR_ARG, "null context");
+  InitArgs a{};
+  a.what = 0; a.sigma = sigma;
+  ctx->eng->init(ctx->b, a, true, false);
+  return launch_check(ctx, "hot_start");
+}
+int gh_cold_start(gh_ctx* ctx) {
+  if (!ctx) return fail(nullptr, GH_ERR_ARG, "null context");
+  InitArgs a{};
+  a.what = 4;
+  ctx->eng->init(ctx->b, a, true, false);
+  return launch_check(ctx, "cold_start");
+}
+int gh_phi_gaussian(gh_ctx* ctx, uint64_t stream, double sigma) {
+  if (!ctx) return fail(nullptr, GH_ERR_ARG, "null context");
+  if (!ctx->scalar) return fail(ctx, GH_ERR_STATE, "no scalar field in a pure-gauge context");
+  InitArgs a{};
+  a.what = 2; a.stream = stream; a.sigma = sigma; a.real = ctx->real; a.d = ctx->d; a.vec = ctx->b.phi;
+  ctx->eng->init(ctx->b, a, false, true);
+  return launch_check(ctx, "phi_gaussian");
+}
+int gh_phi_cold(gh_ctx* ctx, double c) {
+  if (!ctx) return fail(nullptr, GH_ERR_ARG, "null context");
+  if (!ctx->scalar) return fail(ctx, GH_ERR_STATE, "no scalar field in a pure-gauge context");
+  InitArgs a{};
+  a.what = 5; a.sigma = c; a.d = ctx->d; a.vec = ctx->b.phi;
+  ctx->eng->init(ctx->b, a, false, true);
+  return launch_check(ctx, "phi_cold");
+}
+int gh_mom_refresh(gh_ctx* ctx, uint64_t stream) {
+  if (!ctx) return fail(nullptr, GH_ERR_ARG, "null context");
+  InitArgs a{};
+  a.what = 3; a.stream = stream;
+  ctx->eng->init(ctx->b, a, true, false);
+  return launch_check(ctx, "mom_refresh");
+}
+int gh_refresh_momenta(gh_ctx* ctx) {
+  if (!ctx) return fail(nullptr, GH_ERR_ARG, "null context");
+  InitArgs a{};
+  a.what = 1; a.pure = ctx->scalar ? 0 : 1; a.real = ctx->real; a.d = ctx->d; a.vec = ctx->b.pi;
+  ctx->eng->init(ctx->b, a, true, ctx->scalar != 0);
+  return launch_check(ctx, "refresh_momenta");
+}
+
+int gh_gauge_force(gh_ctx* ctx, int lat, double* F) {
+  int rc = check_lat(ctx, lat, false);
+  if (rc) return rc;
+  if (!F) return fail(ctx, GH_ERR_ARG, "null output");
+  ctx->eng->kick(ctx->b, 0.0, M_WRITE, F_GAUGE, ctx->fbuf, true, false);
+  if ((rc = launch_check(ctx, "gauge_force"))) return rc;
+  return xfer_one(ctx, lat, 1, ctx->fbuf, F, false, true);
+}
+int gh_matter_link_force(gh_ctx* ctx, int lat, double* F) {
+  int rc = check_lat(ctx, lat, false);
+  if (rc) return rc;
+  if (!F) return fail(ctx, GH_ERR_ARG, "null output");
+  if (!ctx->scalar) return fail(ctx, GH_ERR_STATE, "no scalar field in a pure-gauge context");
+  if (ctx->rep == REP_GEN) ctx->eng->gen_links(ctx->b, 0.0, 2, ctx->fbuf);
+  else ctx->eng->kick(ctx->b, 0.0, M_WRITE, F_MATTER, ctx->fbuf, true, false);
+  if ((rc = launch_check(ctx, "matter_link_force"))) return rc;
+  return xfer_one(ctx, lat, 1, ctx->fbuf, F, false, true);
+}
+int gh_scalar_force(gh_ctx* ctx, int lat, double* Fphi) {
+  int rc = check_lat(ctx, lat, false);
+  if (rc) return rc;
+  if (!Fphi) return fail(ctx, GH_ERR_ARG, "null output");
+  if (!ctx->scalar) return fail(ctx, GH_ERR_STATE, "no scalar field in a pure-gauge context");
+  if (ctx->rep == REP_GEN) ctx->eng->gen_links(ctx->b, 0.0, 2, ctx->fbuf);
+  ctx->eng->kick(ctx->b, 0.0, M_WRITE, 0, ctx->fphibuf, false, true);
+  if ((rc = launch_check(ctx, "scalar_force"))) return rc;
+  return xfer_one(ctx, lat, 2, ctx->fphibuf, Fphi, false, true);
+}
+
+int gh_kick(gh_ctx* ctx, double eps) {
+  if (!ctx) return fail(nullptr, GH_ERR_ARG, "null context");
+  enq_kick(ctx, eps);
+  return launch_check(ctx, "kick");
+}
+int gh_drift(gh_ctx* ctx, double eps) {
+  if (!ctx) return fail(nullptr, GH_ERR_ARG, "null context");
+  enq_drift(ctx, eps);
+  return launch_check(ctx, "drift");
+}
+int gh_md_evolve(gh_ctx* ctx) {
+  if (!ctx) return fail(nullptr, GH_ERR_ARG, "null context");
+  enq_md(ctx);
+  return launch_check(ctx, "md_evolve");
+}
+int gh_reunitarize(gh_ctx* ctx) {
+  if (!ctx) return fail(nullptr, GH_ERR_ARG, "null context");
+  ctx->eng->reunit(ctx->b);
+  return launch_check(ctx, "reunitarize");
+}
+
+int gh_measure(gh_ctx* ctx, int lat, gh_obs* out) {
+  int rc = check_lat(ctx, lat, true);
+  if (rc) return rc;
+  if (!out) return fail(ctx, GH_ERR_ARG, "null output");
+  enq_measure(ctx, 0);
+  if ((rc = launch_check(ctx, "measure"))) return rc;
+  std::vector<double> res((size_t)ctx->nlat * 2 * NRES);
+  CK(cudaMemcpyAsync(res.data(), ctx->b.res, res.size() * sizeof(double), cudaMemcpyDeviceToHost, ctx->st));
+  CK(cudaStreamSynchronize(ctx->st));
+  const int l0 = lat < 0 ? 0 : lat, l1 = lat < 0 ? ctx->nlat : lat + 1;
+  for (int l = l0; l < l1; ++l) {
+    const double* r = &res[(size_t)l * 2 * NRES];
+    gh_obs& o = out[l - l0];
+    o.H = r[0]; o.S_g = r[1]; o.S_H = r[2]; o.kin_P = r[3]; o.kin_pi = r[4]; o.plaquette = r[5]; o.L_link = r[6]; o.L_phi = r[7];
+  }
+  return GH_OK;
+}
+
+int gh_polyakov(gh_ctx* ctx, int lat, int tdir, double* out) {
+  int rc = check_lat(ctx, lat, true);
+  if (rc) return rc;
+  if (!out) return fail(ctx, GH_ERR_ARG, "null output");
+  if (tdir < 0) tdir = ctx->D - 1;
+  if (tdir >= ctx->D) return fail(ctx, GH_ERR_ARG, "tdir out of range");
+  ctx->eng->polyakov(ctx->b, tdir);
+  if ((rc = launch_check(ctx, "polyakov"))) return rc;
+  std::vector<double> part(ctx->b.nw_sites);
+  CK(cudaMemcpyAsync(part.data(), ctx->b.partials, part.size() * sizeof(double), cudaMemcpyDeviceToHost, ctx->st));
+  CK(cudaStreamSynchronize(ctx->st));
+  // blk_first on the host: site items are laid out per lattice in order
+  int first = 0;
+  const int l0 = lat < 0 ? 0 : lat, l1 = lat < 0 ? ctx->nlat : lat + 1;
+  for (int l = 0; l < ctx->nlat; ++l) {
+    const int nb = (ctx->lat_h[l].V + KBLOCK - 1) / KBLOCK;
+    if (l >= l0 && l < l1) {
+      double s = 0.0;
+      for (int q = first; q < first + nb; ++q) s += part[q];
+      const double count = (double)ctx->lat_h[l].V / ctx->lat_h[l].L[tdir];
+      out[l - l0] = s / (count * ctx->N);
+    }
+    first += nb;
+  }
+  return GH_OK;
+}
+
+int gh_use_graph(gh_ctx* ctx, int enable) {
+  if (!ctx) return fail(nullptr, GH_ERR_ARG, "null context");
+  ctx->use_graph = enable ? 1 : 0;
+  return GH_OK;
+}
+
+int gh_trajectory(gh_ctx* ctx, double* dH, int* accepted) {
+  if (!ctx) return fail(nullptr, GH_ERR_ARG, "null context");
+  int rc = run_traj(ctx);
+  if (rc) return rc;
+  std::vector<LatDev> L(ctx->nlat);
+  std::vector<double> res((size_t)ctx->nlat * 2 * NRES);
+  CK(cudaMemcpyAsync(L.data(), ctx->b.lats, sizeof(LatDev) * ctx->nlat, cudaMemcpyDeviceToHost, ctx->st));
+  CK(cudaMemcpyAsync(res.data(), ctx->b.res, res.size() * sizeof(double), cudaMemcpyDeviceToHost, ctx->st));
+  CK(cudaStreamSynchronize(ctx->st));
+  for (int l = 0; l < ctx->nlat; ++l) {
+    if (dH) dH[l] = res[((size_t)l * 2 + 1) * NRES] - res[(size_t)l * 2 * NRES];
+    if (accepted) accepted[l] = L[l].last_acc;
+  }
+  return GH_OK;
+}
+
+int gh_run_trajectories(gh_ctx* ctx, int ntraj, gh_traj_record* records) {
+  if (!ctx) return fail(nullptr, GH_ERR_ARG, "null context");
+  if (ntraj < 0) return fail(ctx, GH_ERR_ARG, "ntraj < 0");
+  const int cap = ctx->b.hist_cap;
+  std::vector<TrajRec> h((size_t)ctx->nlat * cap);
+  for (int t0 = 0; t0 < ntraj; t0 += cap) {
+    const int nt = std::min(cap, ntraj - t0);
+    for (int t = 0; t < nt; ++t) { int rc = run_traj(ctx); if (rc) return rc; }
+    if (records) {
+      std::vector<LatDev> L(ctx->nlat);
+      CK(cudaMemcpyAsync(L.data(), ctx->b.lats, sizeof(LatDev) * ctx->nlat, cudaMemcpyDeviceToHost, ctx->st));
+      CK(cudaMemcpyAsync(h.data(), ctx->b.hist, sizeof(TrajRec) * h.size(), cudaMemcpyDeviceToHost, ctx->st));
+      CK(cudaStreamSynchronize(ctx->st));
+      for (int l = 0; l < ctx->nlat; ++l)
+        for (int t = 0; t < nt; ++t) {
+          const unsigned long long tr = L[l].traj - (unsigned long long)(nt - t);   // traj number - 1 of record t
+          const TrajRec& r = h[(size_t)l * cap + (int)(tr % (unsigned long long)cap)];
+          gh_traj_record& o = records[(size_t)(t0 + t) * ctx->nlat + l];
+          o.dH = r.dH; o.accepted = r.accepted; o.traj = r.traj; o.plaquette = r.plaq; o.L_phi = r.L_phi; o.L_link = r.L_link;
+        }
+    }
+  }
+  if (!records) CK(cudaStreamSynchronize(ctx->st));
+  return launch_check(ctx, "run_trajectories");
+}
+
+int gh_trajectory_host(gh_ctx* ctx, double* U, double* phi, gh_traj_record* rec) {
+  if (!ctx) return fail(nullptr, GH_ERR_ARG, "null context");
+  if (ctx->nlat != 1) return fail(ctx, GH_ERR_ARG, "gh_trajectory_host needs a single-lattice context");
+  int rc;
+  if (U && (rc = gh_set_links(ctx, 0, U))) return rc;
+  if (phi && ctx->scalar && (rc = gh_set_phi(ctx, 0, phi))) return rc;
+  if ((rc = run_traj(ctx))) return rc;
+  if (U && (rc = gh_get_links(ctx, 0, U))) return rc;
+  if (phi && ctx->scalar && (rc = gh_get_phi(ctx, 0, phi))) return rc;
+  if (rec) {
+    LatDev L;
+    TrajRec r;
+    CK(cudaMemcpyAsync(&L, ctx->b.lats, sizeof(L), cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
+    const int slot = (int)((L.traj - 1) % (unsigned long long)ctx->b.hist_cap);
+    CK(cudaMemcpy(&r, ctx->b.hist + slot, sizeof(r), cudaMemcpyDeviceToHost));
+    rec->dH = r.dH; rec->accepted = r.accepted; rec->traj = r.traj; rec->plaquette = r.plaq; rec->L_phi = r.L_phi; rec->L_link = r.L_link;
+  } else {
+    CK(cudaStreamSynchronize(ctx->st));
+  }
+  return GH_OK;
+}
+
+int gh_temper_enable(gh_ctx* ctx, int mode, uint64_t swap_seed) {
+  if (!ctx) return fail(nullptr, GH_ERR_ARG, "null context");
+  invalidate_graph(ctx);
+  if (mode == 0) { ctx->temper = 0; return GH_OK; }
+  if (!ctx->scalar) return fail(ctx, GH_ERR_STATE, "kappa tempering needs a scalar field");
+  CK(cudaStreamSynchronize(ctx->st));
+  std::vector<LatDev> L(ctx->nlat);
+  CK(cudaMemcpy(L.data(), ctx->b.lats, sizeof(LatDev) * ctx->nlat, cudaMemcpyDeviceToHost));
+  // group lattices by extents, order each group by kappa
+  std::map<std::vector<int>, std::vector<int>> groups;
+  for (int l = 0; l < ctx->nlat; ++l) groups[std::vector<int>(L[l].L, L[l].L + ctx->D)].push_back(l);
+  std::vector<int> order, gb(1, 0), pairmap;
+  for (auto& kv : groups) {
+    auto v = kv.second;
+    std::sort(v.begin(), v.end(), [&](int a, int b) { return L[a].kappa < L[b].kappa; });
+    for (size_t k = 0; k + 1 < v.size(); ++k)
+      if (!(L[v[k + 1]].kappa > L[v[k]].kappa)) return fail(ctx, GH_ERR_ARG, "kappa ladder of equal-extent lattices must be strictly increasing");
+    order.insert(order.end(), v.begin(), v.end());
+    gb.push_back((int)order.size());
+  }
+  // pair id of position k (pair (k, k+1) within a group) -> compact index over all groups
+  pairmap.assign(order.size(), 0);
+  int pid = 0;
+  for (size_t g = 0; g + 1 < gb.size(); ++g)
+    for (int k = gb[g]; k + 1 < gb[g + 1]; ++k) pairmap[k] = pid++;
+  int rc;
+  if (!ctx->t_order) {
+    if ((rc = dalloc(ctx, &ctx->t_order, ctx->nlat)) || (rc = dalloc(ctx, &ctx->t_groups, ctx->nlat + 1)) ||
+        (rc = dalloc(ctx, &ctx->t_stats, 2 * ctx->nlat + 1)) || (rc = dalloc(ctx, &ctx->t_pairmap, ctx->nlat)))
+      return rc;
+  }
+  CK(cudaMemcpy(ctx->t_order, order.data(), sizeof(int) * order.size(), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(ctx->t_groups, gb.data(), sizeof(int) * gb.size(), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(ctx->t_pairmap, pairmap.data(), sizeof(int) * pairmap.size(), cudaMemcpyHostToDevice));
+  CK(cudaMemset(ctx->t_stats, 0, sizeof(unsigned long long) * (2 * ctx->nlat + 1)));
+  ctx->t_ngroups = (int)gb.size() - 1;
+  ctx->temper = mode;
+  ctx->swap_seed = swap_seed;
+  return GH_OK;
+}
+
+int gh_temper_stats(gh_ctx* ctx, uint64_t* attempts, uint64_t* accepts, double* kappa_of_lat) {
+  if (!ctx) return fail(nullptr, GH_ERR_ARG, "null context");
+  CK(cudaStreamSynchronize(ctx->st));
+  if (ctx->t_stats) {
+    std::vector<unsigned long long> s(2 * ctx->nlat + 1);
+    CK(cudaMemcpy(s.data(), ctx->t_stats, sizeof(unsigned long long) * s.size(), cudaMemcpyDeviceToHost));
+    for (int k = 0; k < ctx->nlat - 1; ++k) {
+      if (attempts) attempts[k] = s[k];
+      if (accepts) accepts[k] = s[ctx->nlat + k];
+    }
+  }
+  if (kappa_of_lat) {
+    std::vector<LatDev> L(ctx->nlat);
+    CK(cudaMemcpy(L.data(), ctx->b.lats, sizeof(LatDev) * ctx->nlat, cudaMemcpyDeviceToHost));
+    for (int l = 0; l < ctx->nlat; ++l) kappa_of_lat[l] = L[l].kappa;
+  }
+  return GH_OK;
+}
+
+}  // extern "C"

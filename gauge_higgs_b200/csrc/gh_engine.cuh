@@ -1,0 +1,134 @@
+// gh_engine.cuh -- launchers of one (D, N, precision, representation) instance.
+// The context (gh_ctx.cu) holds one Engine chosen at creation; every launch goes
+// to the context's stream, so a whole trajectory can be captured as a graph.
+#pragma once
+#include "gh_kernels.cuh"
+
+namespace ghk {
+
+struct Bufs {
+  void *U, *Us, *P, *phi, *phis, *pi, *psif, *psib;
+  LatDev* lats;
+  Work* w_all;     // link items (all lattices, all mu) followed by site items
+  int nw_links, nw_sites;
+  Work* w_gen;     // general irrep: items of GEN_WARPS links
+  int nw_gen;
+  int* blk_first;  // [nlat+1] first site item of each lattice (relative to the site items)
+  double* partials;
+  double* res;
+  TrajRec* hist;
+  int hist_cap;
+  GenTables gen;
+  int nlat, D, N, d, rep, scalar;
+  cudaStream_t st;
+};
+
+struct EngineBase {
+  virtual ~EngineBase() {}
+  virtual void kick(const Bufs& b, double eps, int mode, int flags, double* out, bool links, bool sites) = 0;
+  virtual void gen_links(const Bufs& b, double eps, int mode, double* out) = 0;
+  virtual void drift(const Bufs& b, double eps, int reunit) = 0;
+  virtual void reunit(const Bufs& b) = 0;
+  virtual void measure(const Bufs& b) = 0;
+  virtual void init(const Bufs& b, InitArgs a, bool links, bool sites) = 0;
+  virtual void restore(const Bufs& b) = 0;
+  virtual void polyakov(const Bufs& b, int tdir) = 0;
+  virtual void xfer(const Bufs& b, XferArgs a) = 0;
+  virtual size_t gen_smem(const Bufs& b) const = 0;
+  virtual int prepare(const Bufs& b) = 0;
+};
+
+template <int D, int N, typename R, int REP>
+struct Engine : EngineBase {
+  typedef typename Cmp<R>::t C;
+  Engine() {}
+  size_t gen_smem(const Bufs& b) const override {
+    return (size_t)GEN_WARPS * (b.gen.dimT + 4 * b.gen.d) * sizeof(cx<C>);
+  }
+  int prepare(const Bufs& b) override {
+    if (REP != REP_GEN) return 0;
+    const cudaError_t e = cudaFuncSetAttribute(k_gen_links<D, N, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)gen_smem(b));
+    return e == cudaSuccess ? 0 : -1;
+  }
+  void kick(const Bufs& b, double eps, int mode, int flags, double* out, bool links, bool sites) override {
+    KickArgs a;
+    a.lats = b.lats; a.U = b.U; a.P = b.P; a.phi = b.phi; a.pi = b.pi; a.psif = b.psif; a.psib = b.psib;
+    a.eps = eps; a.mode = mode; a.flags = flags; a.d = b.d; a.out = out;
+    const bool do_sites = sites && b.scalar;
+    const int first = links ? 0 : b.nw_links;
+    const int count = (links ? b.nw_links : 0) + (do_sites ? b.nw_sites : 0);
+    if (count == 0) return;
+    a.work = b.w_all + first;
+    k_kick<D, N, R, REP><<<count, KBLOCK, 0, b.st>>>(a);
+  }
+  void gen_links(const Bufs& b, double eps, int mode, double* out) override {
+    if (REP != REP_GEN) return;
+    GenArgs a;
+    a.work = b.w_gen; a.lats = b.lats; a.U = b.U; a.P = b.P; a.phi = b.phi; a.psif = b.psif; a.psib = b.psib;
+    a.t = b.gen; a.eps = eps; a.mode = mode; a.out = out;
+    const size_t sm = gen_smem(b);
+    k_gen_links<D, N, R><<<b.nw_gen, GEN_WARPS * 32, sm, b.st>>>(a);
+  }
+  void drift(const Bufs& b, double eps, int reunit) override {
+    DriftArgs a;
+    a.work = b.w_all; a.lats = b.lats; a.U = b.U; a.P = b.P; a.phi = b.phi; a.pi = b.pi;
+    a.eps = eps; a.reunit = reunit; a.d = b.d;
+    k_drift<N, R><<<b.nw_links + (b.scalar ? b.nw_sites : 0), KBLOCK, 0, b.st>>>(a);
+  }
+  void reunit(const Bufs& b) override {
+    LinkArgs a;
+    a.work = b.w_all; a.lats = b.lats; a.U = b.U; a.Us = b.Us;
+    k_reunit<N, R><<<b.nw_links, KBLOCK, 0, b.st>>>(a);
+  }
+  void measure(const Bufs& b) override {
+    if (REP == REP_GEN && b.scalar) gen_links(b, 0.0, 1, nullptr);
+    MeasArgs a;
+    a.work = b.w_all + b.nw_links; a.lats = b.lats; a.U = b.U; a.P = b.P; a.phi = b.phi; a.pi = b.pi;
+    a.psif = b.psif; a.d = b.d; a.scalar = b.scalar; a.partials = b.partials;
+    k_measure<D, N, R, REP><<<b.nw_sites, KBLOCK, 0, b.st>>>(a);
+  }
+  void init(const Bufs& b, InitArgs a, bool links, bool sites) override {
+    a.lats = b.lats; a.U = b.U; a.P = b.P;
+    const int first = links ? 0 : b.nw_links;
+    const int count = (links ? b.nw_links : 0) + (sites ? b.nw_sites : 0);
+    if (count == 0) return;
+    a.work = b.w_all + first;
+    k_init<N, R><<<count, KBLOCK, 0, b.st>>>(a);
+  }
+  void restore(const Bufs& b) override {
+    RestoreArgs a;
+    a.work = b.w_all; a.lats = b.lats; a.U = b.U; a.Us = b.Us; a.phi = b.phi; a.phis = b.phis; a.N = N; a.d = b.d;
+    k_restore<R><<<b.nw_links + (b.scalar ? b.nw_sites : 0), KBLOCK, 0, b.st>>>(a);
+  }
+  void polyakov(const Bufs& b, int tdir) override {
+    PolyArgs a;
+    a.work = b.w_all + b.nw_links; a.lats = b.lats; a.U = b.U; a.tdir = tdir; a.partials = b.partials;
+    k_polyakov<D, N, R><<<b.nw_sites, KBLOCK, 0, b.st>>>(a);
+  }
+  void xfer(const Bufs& b, XferArgs a) override {
+    a.lats = b.lats;
+    k_xfer<R><<<296, 256, 0, b.st>>>(a);
+  }
+};
+
+// Factories, one per (N, precision) translation unit.
+EngineBase* make_engine_n2_f64(int D, int rep);
+EngineBase* make_engine_n2_f32(int D, int rep);
+EngineBase* make_engine_n3_f64(int D, int rep);
+EngineBase* make_engine_n3_f32(int D, int rep);
+
+template <int N, typename R>
+EngineBase* make_engine_NR(int D, int rep) {
+#define GH_MK(DD) \
+  switch (rep) { case REP_NONE: return new Engine<DD, N, R, REP_NONE>(); case REP_FUND: return new Engine<DD, N, R, REP_FUND>(); \
+    case REP_ADJ: return new Engine<DD, N, R, REP_ADJ>(); case REP_GEN: return new Engine<DD, N, R, REP_GEN>(); default: return nullptr; }
+  switch (D) {
+    case 2: GH_MK(2)
+    case 3: GH_MK(3)
+    case 4: GH_MK(4)
+    default: return nullptr;
+  }
+#undef GH_MK
+}
+
+}  // namespace ghk

@@ -1,0 +1,5 @@
+// Instantiates the kernels of SU(3) in double storage for D = 2, 3, 4 and every representation kind.
+#include "gh_engine.cuh"
+namespace ghk {
+EngineBase* make_engine_n3_f64(int D, int rep) { return make_engine_NR<3, double>(D, rep); }
+}  // namespace ghk

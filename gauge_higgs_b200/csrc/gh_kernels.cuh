@@ -1,0 +1,865 @@
+// gh_kernels.cuh -- sm_100a kernels of the gauge + Higgs molecular-dynamics path.
+//
+// Device layout (component-major SoA, one plane per matrix/vector component so
+// a warp's load of one component for 32 consecutive sites is one 512 B (FP64)
+// or 256 B (FP32) coalesced transaction; complex = {re,im} vector load):
+//   U   [lat][mu][i*N+j][site]   complex R     (reference: [site*D+mu] N x N, src/core/fields.hpp:12-20)
+//   P   [lat][mu][a][site]       real R        (reference: [site*D+mu][a], src/core/fields.hpp:46-57)
+//   phi [lat][k][site]           complex R     (reference: [site*d+k], src/core/scalar_field.hpp:15)
+// R = double (FP64 mode) or float (FP32-MD mode).  Several lattices of unequal
+// extents live back to back; every kernel walks a table of Work items (lattice,
+// direction, first site, count), one per block, so a single launch covers all
+// lattices of a batch.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include "gh_math.cuh"
+#include "gh_rng.cuh"
+
+namespace ghk {
+using namespace ghm;
+
+enum { REP_NONE = 0, REP_FUND = 1, REP_ADJ = 2, REP_GEN = 3 };
+enum { F_GAUGE = 1, F_MATTER = 2 };
+enum { M_UPDATE = 0, M_WRITE = 1 };
+constexpr int KBLOCK = 128;    // threads per block of site/link kernels
+constexpr int GEN_WARPS = 4;   // warps per block of the general-irrep kernel
+constexpr int NRED = 6;        // per-site partial sums of the measure kernel
+
+struct LatDev {
+  int L[4];
+  int stride[4];
+  int V;
+  int cidx;                      // coupling index (tempering bookkeeping)
+  long long u_off, p_off, f_off, g_off;  // complex / real / complex / complex element offsets
+  double beta, kappa, lambda;
+  unsigned long long seed;
+  unsigned long long traj, accepted, nonfinite;
+  int last_acc;
+  int pad;
+};
+struct Work { int lat, mu, s0, n; };   // mu = -1: site item
+
+struct GenTables {                 // general irrep (src/rep/rep_general.hpp), sparse
+  int d, n, dimT, ng;
+  int powN[16];
+  const int* wt_ptr; const int* wt_l; const double2* wt_v;   // lift: CSR over tensor index
+  const int* w_ptr;  const int* w_i;  const double2* w_v;    // project: CSR over basis vector
+  const int* t_ptr;  const int* t_j;  const double2* t_v;    // T^a_R: CSR over (a, row)
+};
+
+template <typename R> struct V2;
+template <> struct V2<double> { typedef double2 t; };
+template <> struct V2<float> { typedef float2 t; };
+template <typename R> struct Cmp { typedef R t; };
+
+template <typename C, typename R> __device__ __forceinline__ cx<C> ldc(const R* __restrict__ p, long long i) {
+  const typename V2<R>::t v = __ldg(reinterpret_cast<const typename V2<R>::t*>(p) + i);
+  return mk<C>((C)v.x, (C)v.y);
+}
+template <typename C, typename R> __device__ __forceinline__ cx<C> ldc_rw(const R* p, long long i) {
+  const typename V2<R>::t v = reinterpret_cast<const typename V2<R>::t*>(p)[i];
+  return mk<C>((C)v.x, (C)v.y);
+}
+template <typename C, typename R> __device__ __forceinline__ void stc(R* p, long long i, cx<C> z) {
+  typename V2<R>::t v;
+  v.x = (R)z.re;
+  v.y = (R)z.im;
+  reinterpret_cast<typename V2<R>::t*>(p)[i] = v;
+}
+template <int N, typename C, typename R>
+__device__ __forceinline__ Mat<N, C> ld_link(const R* __restrict__ U, const LatDev& L, int mu, int s) {
+  Mat<N, C> M;
+  const long long base = L.u_off + (long long)mu * N * N * L.V + s;
+#pragma unroll
+  for (int c = 0; c < N * N; ++c) M.e[c] = ldc<C>(U, base + (long long)c * L.V);
+  return M;
+}
+template <int N, typename C, typename R>
+__device__ __forceinline__ Mat<N, C> ld_link_rw(const R* U, const LatDev& L, int mu, int s) {
+  Mat<N, C> M;
+  const long long base = L.u_off + (long long)mu * N * N * L.V + s;
+#pragma unroll
+  for (int c = 0; c < N * N; ++c) M.e[c] = ldc_rw<C>(U, base + (long long)c * L.V);
+  return M;
+}
+template <int N, typename C, typename R>
+__device__ __forceinline__ void st_link(R* U, const LatDev& L, int mu, int s, const Mat<N, C>& M) {
+  const long long base = L.u_off + (long long)mu * N * N * L.V + s;
+#pragma unroll
+  for (int c = 0; c < N * N; ++c) stc<C>(U, base + (long long)c * L.V, M.e[c]);
+}
+
+template <int D> __device__ __forceinline__ void coords(const LatDev& L, int s, int* x) {
+  int r = s;
+#pragma unroll
+  for (int mu = 0; mu < D; ++mu) { x[mu] = r % L.L[mu]; r /= L.L[mu]; }
+}
+// neighbour of site s (whose coordinate in direction mu is xm) in +mu / -mu
+__device__ __forceinline__ int nfwd(const LatDev& L, int s, int xm, int mu) {
+  return (xm + 1 < L.L[mu]) ? s + L.stride[mu] : s - xm * L.stride[mu];
+}
+__device__ __forceinline__ int nbwd(const LatDev& L, int s, int xm, int mu) {
+  return (xm > 0) ? s - L.stride[mu] : s + (L.L[mu] - 1) * L.stride[mu];
+}
+
+// ---------------------------------------------------------------------------
+// Representation apply for the register-resident reps.
+// Fundamental: D(U) = U (src/rep/rep_fundamental.hpp:15-25).
+// Adjoint: D_ab = 2 Re Tr(T^a U T^b U^dag) (src/rep/rep_adjoint.hpp:27-40) applied
+// without forming D: (D phi)_a = 2 Tr(T^a U Phi U^dag), Phi = sum_b phi_b T^b.
+// ---------------------------------------------------------------------------
+template <int N, typename C>
+__device__ __forceinline__ void fund_apply(const Mat<N, C>& U, const cx<C>* v, cx<C>* o, bool dag) {
+#pragma unroll
+  for (int i = 0; i < N; ++i) {
+    cx<C> s = dag ? cmul(U.e[i], v[0]) : mul(U.e[i * N], v[0]);
+#pragma unroll
+    for (int j = 1; j < N; ++j) s = add(s, dag ? cmul(U.e[j * N + i], v[j]) : mul(U.e[i * N + j], v[j]));
+    o[i] = s;
+  }
+}
+template <int N, typename C>
+__device__ __forceinline__ void adj_apply(const Mat<N, C>& U, const cx<C>* v, cx<C>* o, bool dag) {
+  const Mat<N, C> Phi = alg_to_mat_c<N, C>(v);
+  Mat<N, C> Psi = dag ? mm(mm_dn(U, Phi), U) : mm_nd(mm(U, Phi), U);
+  tr2_proj<N, C>(Psi, o);
+}
+
+template <int N, int REP> struct RepDim { static constexpr int d = (REP == REP_FUND) ? N : (REP == REP_ADJ) ? N * N - 1 : 1; };
+
+// ---------------------------------------------------------------------------
+// Kick: link items (gauge force + matter back-reaction, P -= eps F) and site
+// items (scalar force, pi += eps F_phi) of one launch.
+//   gauge force  F^a = (beta/N) Im Tr(T^a U Sigma)      src/action/gauge_wilson.hpp:11-27,70-83
+//   matter force F^a = -kappa g^a                        src/action/scalar_higgs.hpp:113-128
+//   scalar force F_phi = -2 dV/dphi* + 2 kappa sum_mu [D phi_{x+mu} + D^dag phi_{x-mu}]
+//                                                        src/action/scalar_higgs.hpp:71-108
+// Fundamental rep: -kappa g^a = 2 kappa Im Tr(T^a psi phi_x^dag), psi = U phi_{x+mu},
+// so one projection of (beta/N) U Sigma + 2 kappa psi phi_x^dag gives the total link force.
+// Adjoint rep: -kappa g^a = -4 kappa Im Tr(T^a [conj(Phi_x), U Phi_y U^dag]).
+// ---------------------------------------------------------------------------
+struct KickArgs {
+  const Work* work;
+  const LatDev* lats;
+  const void* U;
+  void* P;
+  const void* phi;
+  void* pi;
+  const void* psif;   // general irrep scratch: D(U_mu(x)) phi_{x+mu}
+  const void* psib;   // general irrep scratch: D(U_mu(x))^dag phi_x
+  double eps;
+  int mode;           // M_UPDATE or M_WRITE
+  int flags;          // F_GAUGE | F_MATTER
+  int d;              // rep dimension (general irreps)
+  double* out;        // M_WRITE destination (SoA like P / like phi, FP64)
+};
+
+template <int D, int N, typename R, int REP>
+__device__ __forceinline__ void kick_link(const KickArgs& a, const LatDev& L, int mu, int s) {
+  typedef typename Cmp<R>::t C;
+  const R* U = (const R*)a.U;
+  int x[D];
+  coords<D>(L, s, x);
+  const int spm = nfwd(L, s, x[mu], mu);
+  const Mat<N, C> Umu = ld_link<N, C>(U, L, mu, s);
+  Mat<N, C> Om;
+  set_zero(Om);
+  if (a.flags & F_GAUGE) {
+    Mat<N, C> sig;
+    set_zero(sig);
+#pragma unroll
+    for (int nu = 0; nu < D; ++nu) {
+      if (nu == mu) continue;
+      const int spn = nfwd(L, s, x[nu], nu);
+      const int smn = nbwd(L, s, x[nu], nu);
+      const int spm_mn = nbwd(L, spm, x[nu], nu);
+      {
+        Mat<N, C> A = mm_nd(ld_link<N, C>(U, L, nu, spm), ld_link<N, C>(U, L, mu, spn));
+        A = mm_nd(A, ld_link<N, C>(U, L, nu, s));
+        acc(sig, A);
+      }
+      {
+        Mat<N, C> B = mm_dd(ld_link<N, C>(U, L, nu, spm_mn), ld_link<N, C>(U, L, mu, smn));
+        B = mm(B, ld_link<N, C>(U, L, nu, smn));
+        acc(sig, B);
+      }
+    }
+    Om = mm(Umu, sig);
+    const C c = (C)(L.beta / N);
+#pragma unroll
+    for (int i = 0; i < N * N; ++i) Om.e[i] = scale(Om.e[i], c);
+  }
+  if ((a.flags & F_MATTER) && (REP == REP_FUND || REP == REP_ADJ)) {
+    constexpr int d = RepDim<N, REP>::d;
+    const R* phi = (const R*)a.phi;
+    cx<C> px[d], py[d];
+#pragma unroll
+    for (int k = 0; k < d; ++k) {
+      px[k] = ldc<C>(phi, L.f_off + (long long)k * L.V + s);
+      py[k] = ldc<C>(phi, L.f_off + (long long)k * L.V + spm);
+    }
+    const C kap = (C)L.kappa;
+    if (REP == REP_FUND) {
+      cx<C> psi[N];
+      fund_apply<N, C>(Umu, py, psi, false);
+      const C k2 = C(2) * kap;
+#pragma unroll
+      for (int i = 0; i < N; ++i)
+#pragma unroll
+        for (int j = 0; j < N; ++j) Om.e[i * N + j] = add(Om.e[i * N + j], scale(mulc(psi[i], px[j]), k2));
+    } else {
+      cx<C> pxc[d];
+#pragma unroll
+      for (int k = 0; k < d; ++k) pxc[k] = conj(px[k]);
+      const Mat<N, C> Phx = alg_to_mat_c<N, C>(pxc);
+      const Mat<N, C> Psi = mm_nd(mm(Umu, alg_to_mat_c<N, C>(py)), Umu);
+      const Mat<N, C> c1 = mm(Phx, Psi), c2 = mm(Psi, Phx);
+      const C k4 = C(-4) * kap;
+#pragma unroll
+      for (int i = 0; i < N * N; ++i) Om.e[i] = add(Om.e[i], scale(sub(c1.e[i], c2.e[i]), k4));
+    }
+  }
+  C F[N * N - 1];
+  im_tr_proj<N, C>(Om, F);
+  constexpr int ng = N * N - 1;
+  const long long pb = L.p_off + (long long)mu * ng * L.V + s;
+  if (a.mode == M_UPDATE) {
+    R* P = (R*)a.P;
+    const C eps = (C)a.eps;
+#pragma unroll
+    for (int g = 0; g < ng; ++g) P[pb + (long long)g * L.V] = (R)((C)P[pb + (long long)g * L.V] - eps * F[g]);
+  } else {
+#pragma unroll
+    for (int g = 0; g < ng; ++g) a.out[pb + (long long)g * L.V] = (double)F[g];
+  }
+}
+
+template <int D, int N, typename R, int REP>
+__device__ __forceinline__ void kick_site(const KickArgs& a, const LatDev& L, int s) {
+  typedef typename Cmp<R>::t C;
+  const R* U = (const R*)a.U;
+  const R* phi = (const R*)a.phi;
+  int x[D];
+  coords<D>(L, s, x);
+  const C kap2 = C(2) * (C)L.kappa;
+  if (REP == REP_FUND || REP == REP_ADJ) {
+    constexpr int d = RepDim<N, REP>::d;
+    cx<C> F[d], v[d], o[d];
+    C n2 = C(0);
+#pragma unroll
+    for (int k = 0; k < d; ++k) { v[k] = ldc<C>(phi, L.f_off + (long long)k * L.V + s); n2 += norm2(v[k]); }
+    const C cc = C(1) + C(2) * (C)L.lambda * (n2 - C(1));
+#pragma unroll
+    for (int k = 0; k < d; ++k) F[k] = scale(v[k], C(-2) * cc);
+#pragma unroll
+    for (int mu = 0; mu < D; ++mu) {
+      const int yf = nfwd(L, s, x[mu], mu), yb = nbwd(L, s, x[mu], mu);
+      cx<C> o2[d];
+#pragma unroll
+      for (int k = 0; k < d; ++k) v[k] = ldc<C>(phi, L.f_off + (long long)k * L.V + yf);
+      {
+        const Mat<N, C> Uf = ld_link<N, C>(U, L, mu, s);
+        if (REP == REP_FUND) fund_apply<N, C>(Uf, v, o, false); else adj_apply<N, C>(Uf, v, o, false);
+      }
+#pragma unroll
+      for (int k = 0; k < d; ++k) v[k] = ldc<C>(phi, L.f_off + (long long)k * L.V + yb);
+      {
+        const Mat<N, C> Ub = ld_link<N, C>(U, L, mu, yb);
+        if (REP == REP_FUND) fund_apply<N, C>(Ub, v, o2, true); else adj_apply<N, C>(Ub, v, o2, true);
+      }
+#pragma unroll
+      for (int k = 0; k < d; ++k) F[k] = add(F[k], scale(add(o[k], o2[k]), kap2));
+    }
+    const long long fb = L.f_off + s;
+    if (a.mode == M_UPDATE) {
+      R* pi = (R*)a.pi;
+      const C eps = (C)a.eps;
+#pragma unroll
+      for (int k = 0; k < d; ++k) stc<C>(pi, fb + (long long)k * L.V, add(ldc_rw<C>(pi, fb + (long long)k * L.V), scale(F[k], eps)));
+    } else {
+      double2* out = reinterpret_cast<double2*>(a.out);
+#pragma unroll
+      for (int k = 0; k < d; ++k) out[fb + (long long)k * L.V] = make_double2((double)F[k].re, (double)F[k].im);
+    }
+  } else if (REP == REP_GEN) {
+    const int d = a.d;
+    const R* psif = (const R*)a.psif;
+    const R* psib = (const R*)a.psib;
+    C n2 = C(0);
+    for (int k = 0; k < d; ++k) n2 += norm2(ldc<C>(phi, L.f_off + (long long)k * L.V + s));
+    const C cc = C(1) + C(2) * (C)L.lambda * (n2 - C(1));
+    int yb[D];
+#pragma unroll
+    for (int mu = 0; mu < D; ++mu) yb[mu] = nbwd(L, s, x[mu], mu);
+    for (int k = 0; k < d; ++k) {
+      cx<C> F = scale(ldc<C>(phi, L.f_off + (long long)k * L.V + s), C(-2) * cc);
+#pragma unroll
+      for (int mu = 0; mu < D; ++mu) {
+        const long long gb = L.g_off + ((long long)mu * d + k) * L.V;
+        F = add(F, scale(add(ldc<C>(psif, gb + s), ldc<C>(psib, gb + yb[mu])), kap2));
+      }
+      const long long fi = L.f_off + (long long)k * L.V + s;
+      if (a.mode == M_UPDATE) {
+        R* pi = (R*)a.pi;
+        stc<C>(pi, fi, add(ldc_rw<C>(pi, fi), scale(F, (C)a.eps)));
+      } else {
+        reinterpret_cast<double2*>(a.out)[fi] = make_double2((double)F.re, (double)F.im);
+      }
+    }
+  }
+}
+
+template <int D, int N, typename R, int REP>
+__global__ void __launch_bounds__(KBLOCK) k_kick(const KickArgs a) {
+  const Work w = a.work[blockIdx.x];
+  if ((int)threadIdx.x >= w.n) return;
+  const LatDev L = a.lats[w.lat];
+  const int s = w.s0 + threadIdx.x;
+  if (w.mu >= 0) kick_link<D, N, R, REP>(a, L, w.mu, s);
+  else if (REP != REP_NONE) kick_site<D, N, R, REP>(a, L, s);
+}
+
+// ---------------------------------------------------------------------------
+// General irrep: one warp per link.  D^(R)(U) phi is applied matrix-free on the
+// tensor space V^{xn} exactly as src/rep/rep_general.hpp:184-220 does (lift with
+// the basis W, apply U on each of the n slots, project with W^dag), but W and
+// T^a_R are held sparse (97% / 94% zeros for the SU(3) 27-plet) and the lanes of
+// the warp split the tensor index / slot fibres / basis vectors between them.
+//   mode 0: psi_f = D phi_{x+mu}, psi_b = D^dag phi_x -> scratch; P -= eps F_matter
+//   mode 1: psi_f only (for the scalar action and the link energy)
+//   mode 2: F_matter -> out (no P update), psi_f, psi_b -> scratch
+// hop_link_g: src/rep/representation.hpp:36-46 / rep_general.hpp:151-159.
+// ---------------------------------------------------------------------------
+struct GenArgs {
+  const Work* work;
+  const LatDev* lats;
+  const void* U;
+  void* P;
+  const void* phi;
+  void* psif;
+  void* psib;
+  GenTables t;
+  double eps;
+  int mode;
+  double* out;
+};
+
+template <int N, typename C>
+__device__ void gen_apply(const GenTables& t, const Mat<N, C>& M, bool dag, const cx<C>* vin, cx<C>* buf,
+                          cx<C>* vout, int lane) {
+  // lift: buf[i] = sum_l vin[l] W_l[i]
+  for (int i = lane; i < t.dimT; i += 32) {
+    cx<C> s = zero<C>();
+    for (int p = t.wt_ptr[i]; p < t.wt_ptr[i + 1]; ++p) {
+      const double2 w = t.wt_v[p];
+      s = add(s, mul(vin[t.wt_l[p]], mk<C>((C)w.x, (C)w.y)));
+    }
+    buf[i] = s;
+  }
+  __syncwarp();
+  // slot applies: fibre f of slot sl holds the N entries base + j*blk
+  const int nf = t.dimT / N;
+  for (int sl = 0; sl < t.n; ++sl) {
+    const int blk = t.powN[t.n - 1 - sl];
+    for (int f = lane; f < nf; f += 32) {
+      const int base = (f / blk) * blk * N + (f % blk);
+      cx<C> v[N];
+#pragma unroll
+      for (int j = 0; j < N; ++j) v[j] = buf[base + j * blk];
+#pragma unroll
+      for (int j = 0; j < N; ++j) {
+        cx<C> s = dag ? cmul(M.e[j], v[0]) : mul(M.e[j * N], v[0]);
+#pragma unroll
+        for (int g = 1; g < N; ++g) s = add(s, dag ? cmul(M.e[g * N + j], v[g]) : mul(M.e[j * N + g], v[g]));
+        buf[base + j * blk] = s;
+      }
+    }
+    __syncwarp();
+  }
+  // project: vout[k] = sum_i conj(W_k[i]) buf[i]
+  for (int k = lane; k < t.d; k += 32) {
+    cx<C> s = zero<C>();
+    for (int p = t.w_ptr[k]; p < t.w_ptr[k + 1]; ++p) {
+      const double2 w = t.w_v[p];
+      s = add(s, cmul(mk<C>((C)w.x, (C)w.y), buf[t.w_i[p]]));
+    }
+    vout[k] = s;
+  }
+  __syncwarp();
+}
+
+template <int D, int N, typename R>
+__global__ void __launch_bounds__(GEN_WARPS * 32) k_gen_links(const GenArgs a) {
+  typedef typename Cmp<R>::t C;
+  extern __shared__ unsigned char smem_raw[];
+  const Work w = a.work[blockIdx.x];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (warp >= w.n) return;
+  const LatDev L = a.lats[w.lat];
+  const int mu = w.mu, s = w.s0 + warp;
+  const int d = a.t.d, dimT = a.t.dimT;
+  cx<C>* base = reinterpret_cast<cx<C>*>(smem_raw) + (size_t)warp * (dimT + 4 * d);
+  cx<C>* buf = base;
+  cx<C>* px = buf + dimT;
+  cx<C>* py = px + d;
+  cx<C>* pf = py + d;
+  cx<C>* pb = pf + d;
+  const R* U = (const R*)a.U;
+  const R* phi = (const R*)a.phi;
+  int x[D];
+  coords<D>(L, s, x);
+  const int spm = nfwd(L, s, x[mu], mu);
+  const Mat<N, C> M = ld_link<N, C>(U, L, mu, s);
+  for (int k = lane; k < d; k += 32) {
+    px[k] = ldc<C>(phi, L.f_off + (long long)k * L.V + s);
+    py[k] = ldc<C>(phi, L.f_off + (long long)k * L.V + spm);
+  }
+  __syncwarp();
+  gen_apply<N, C>(a.t, M, false, py, buf, pf, lane);
+  if (a.mode != 1) gen_apply<N, C>(a.t, M, true, px, buf, pb, lane);
+  R* psif = (R*)a.psif;
+  R* psib = (R*)a.psib;
+  for (int k = lane; k < d; k += 32) {
+    const long long gi = L.g_off + ((long long)mu * d + k) * L.V + s;
+    stc<C>(psif, gi, pf[k]);
+    if (a.mode != 1) stc<C>(psib, gi, pb[k]);
+  }
+  if (a.mode == 1) return;
+  // matter force: g^a = -2 Im(phi_x^dag T^a_R psi_f), F^a = -kappa g^a
+  constexpr int ng = N * N - 1;
+  for (int g = lane; g < ng; g += 32) {
+    cx<C> z = zero<C>();
+    for (int i = 0; i < d; ++i) {
+      cx<C> ti = zero<C>();
+      const int r = g * d + i;
+      for (int p = a.t.t_ptr[r]; p < a.t.t_ptr[r + 1]; ++p) {
+        const double2 tv = a.t.t_v[p];
+        ti = add(ti, mul(mk<C>((C)tv.x, (C)tv.y), pf[a.t.t_j[p]]));
+      }
+      z = add(z, cmul(px[i], ti));
+    }
+    const C F = -(C)L.kappa * (C(-2) * z.im);
+    const long long pi_ = L.p_off + ((long long)mu * ng + g) * L.V + s;
+    if (a.mode == 0) {
+      R* P = (R*)a.P;
+      P[pi_] = (R)((C)P[pi_] - (C)a.eps * F);
+    } else {
+      a.out[pi_] = (double)F;
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Drift: U <- exp(i eps P) U (src/hmc/gauge_higgs_hmc.hpp:136-143), with the
+// exponential and the product in FP64; optional reunitarisation (FP32-MD mode
+// reunitarises every step).  Site items: phi += eps pi (:145-146).
+// ---------------------------------------------------------------------------
+struct DriftArgs {
+  const Work* work;
+  const LatDev* lats;
+  void* U;
+  const void* P;
+  void* phi;
+  const void* pi;
+  double eps;
+  int reunit;
+  int d;
+};
+template <int N, typename R>
+__global__ void __launch_bounds__(KBLOCK) k_drift(const DriftArgs a) {
+  const Work w = a.work[blockIdx.x];
+  if ((int)threadIdx.x >= w.n) return;
+  const LatDev L = a.lats[w.lat];
+  const int s = w.s0 + threadIdx.x;
+  if (w.mu >= 0) {
+    const int mu = w.mu;
+    constexpr int ng = N * N - 1;
+    const R* P = (const R*)a.P;
+    double v[ng];
+    const long long pb = L.p_off + (long long)mu * ng * L.V + s;
+#pragma unroll
+    for (int g = 0; g < ng; ++g) v[g] = (double)P[pb + (long long)g * L.V];
+    Mat<N, double> H = alg_to_mat<N, double>(v);
+#pragma unroll
+    for (int i = 0; i < N * N; ++i) H.e[i] = scale(H.e[i], a.eps);
+    const Mat<N, double> E = expi<N>(H);
+    Mat<N, double> Un = mm(E, ld_link_rw<N, double>((const R*)a.U, L, mu, s));
+    if (a.reunit) reunitarize<N, double>(Un);
+    st_link<N, double>((R*)a.U, L, mu, s, Un);
+  } else {
+    typedef typename Cmp<R>::t C;
+    R* phi = (R*)a.phi;
+    const R* pi = (const R*)a.pi;
+    for (int k = 0; k < a.d; ++k) {
+      const long long i = L.f_off + (long long)k * L.V + s;
+      stc<C>(phi, i, add(ldc_rw<C>(phi, i), scale(ldc<C>(pi, i), (C)a.eps)));
+    }
+  }
+}
+
+// Reunitarise all links (src/core/fields.hpp:36, src/group/sun.hpp:48-71), FP64.
+struct LinkArgs { const Work* work; const LatDev* lats; void* U; const void* Us; };
+template <int N, typename R>
+__global__ void __launch_bounds__(KBLOCK) k_reunit(const LinkArgs a) {
+  const Work w = a.work[blockIdx.x];
+  if ((int)threadIdx.x >= w.n || w.mu < 0) return;
+  const LatDev L = a.lats[w.lat];
+  const int s = w.s0 + threadIdx.x;
+  Mat<N, double> M = ld_link_rw<N, double>((const R*)a.U, L, w.mu, s);
+  reunitarize<N, double>(M);
+  st_link<N, double>((R*)a.U, L, w.mu, s, M);
+}
+
+// ---------------------------------------------------------------------------
+// Measure: one pass over sites producing the six per-site sums behind
+// H = 1/2 sum P^2 + 1/2 sum |pi|^2 + S_g + S_H (src/hmc/gauge_higgs_hmc.hpp:105-110)
+// and the observables plaquette, L_link, L_phi (src/action/gauge_wilson.hpp:31-65,
+// src/action/scalar_higgs.hpp:43-65,132-154), all accumulated in FP64:
+//   r0 sum_{mu<nu} Re Tr U_pl   r1 sum V(phi)   r2 sum_mu Re phi_x^dag D phi_{x+mu}
+//   r3 sum P^2                  r4 sum |pi|^2   r5 sum |phi|^2
+// Warp-shuffle tree reduction, then one partial per block (deterministic order).
+// ---------------------------------------------------------------------------
+struct MeasArgs {
+  const Work* work;
+  const LatDev* lats;
+  const void* U;
+  const void* P;
+  const void* phi;
+  const void* pi;
+  const void* psif;
+  int d;
+  int scalar;
+  double* partials;   // [block][NRED]
+};
+
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  return v;
+}
+
+template <int D, int N, typename R, int REP>
+__global__ void __launch_bounds__(KBLOCK) k_measure(const MeasArgs a) {
+  const Work w = a.work[blockIdx.x];
+  double r[NRED] = {0, 0, 0, 0, 0, 0};
+  if ((int)threadIdx.x < w.n) {
+    const LatDev L = a.lats[w.lat];
+    const int s = w.s0 + threadIdx.x;
+    const R* U = (const R*)a.U;
+    int x[D];
+    coords<D>(L, s, x);
+    // plaquettes: Re Tr(U_mu(x) U_nu(x+mu) U_mu(x+nu)^dag U_nu(x)^dag) = Re Tr(A B^dag)
+#pragma unroll
+    for (int mu = 0; mu < D; ++mu) {
+      const int spm = nfwd(L, s, x[mu], mu);
+      const Mat<N, double> Umu = ld_link<N, double>(U, L, mu, s);
+#pragma unroll
+      for (int nu = mu + 1; nu < D; ++nu) {
+        const int spn = nfwd(L, s, x[nu], nu);
+        const Mat<N, double> A = mm(Umu, ld_link<N, double>(U, L, nu, spm));
+        const Mat<N, double> B = mm(ld_link<N, double>(U, L, nu, s), ld_link<N, double>(U, L, mu, spn));
+        r[0] += retr_nd(A, B);
+      }
+    }
+    constexpr int ng = N * N - 1;
+    const R* P = (const R*)a.P;
+#pragma unroll
+    for (int mu = 0; mu < D; ++mu)
+#pragma unroll
+      for (int g = 0; g < ng; ++g) {
+        const double p = (double)P[L.p_off + ((long long)mu * ng + g) * L.V + s];
+        r[3] += p * p;
+      }
+    if (a.scalar) {
+      const R* phi = (const R*)a.phi;
+      const R* pi = (const R*)a.pi;
+      double n2 = 0.0;
+      for (int k = 0; k < a.d; ++k) {
+        n2 += norm2(ldc<double>(phi, L.f_off + (long long)k * L.V + s));
+        r[4] += norm2(ldc<double>(pi, L.f_off + (long long)k * L.V + s));
+      }
+      r[5] = n2;
+      r[1] = n2 + L.lambda * (n2 - 1.0) * (n2 - 1.0);
+      if (REP == REP_FUND || REP == REP_ADJ) {
+        constexpr int d = RepDim<N, REP>::d;
+        cx<double> px[d], py[d], o[d];
+#pragma unroll
+        for (int k = 0; k < d; ++k) px[k] = ldc<double>(phi, L.f_off + (long long)k * L.V + s);
+#pragma unroll
+        for (int mu = 0; mu < D; ++mu) {
+          const int y = nfwd(L, s, x[mu], mu);
+#pragma unroll
+          for (int k = 0; k < d; ++k) py[k] = ldc<double>(phi, L.f_off + (long long)k * L.V + y);
+          const Mat<N, double> Umu = ld_link<N, double>(U, L, mu, s);
+          if (REP == REP_FUND) fund_apply<N, double>(Umu, py, o, false); else adj_apply<N, double>(Umu, py, o, false);
+          double h = 0.0;
+#pragma unroll
+          for (int k = 0; k < d; ++k) h += px[k].re * o[k].re + px[k].im * o[k].im;
+          r[2] += h;
+        }
+      } else if (REP == REP_GEN) {
+        const R* psif = (const R*)a.psif;
+#pragma unroll
+        for (int mu = 0; mu < D; ++mu) {
+          double h = 0.0;
+          for (int k = 0; k < a.d; ++k) {
+            const cx<double> p = ldc<double>(phi, L.f_off + (long long)k * L.V + s);
+            const cx<double> o = ldc<double>(psif, L.g_off + ((long long)mu * a.d + k) * L.V + s);
+            h += p.re * o.re + p.im * o.im;
+          }
+          r[2] += h;
+        }
+      }
+    }
+  }
+  __shared__ double red[KBLOCK / 32][NRED];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int k = 0; k < NRED; ++k) {
+    const double v = warp_sum(r[k]);
+    if (lane == 0) red[warp][k] = v;
+  }
+  __syncthreads();
+  if (threadIdx.x < NRED) {
+    double v = 0.0;
+#pragma unroll
+    for (int q = 0; q < KBLOCK / 32; ++q) v += red[q][threadIdx.x];
+    a.partials[(size_t)blockIdx.x * NRED + threadIdx.x] = v;
+  }
+}
+
+// Per-lattice totals of the measure partials and the derived quantities.
+// res[l][slot][k]: 0 H, 1 S_g, 2 S_H, 3 kin_P, 4 kin_pi, 5 plaquette, 6 L_link, 7 L_phi
+constexpr int NRES = 8;
+struct FinArgs {
+  const LatDev* lats;
+  const int* blk_first;   // [nlat+1] block range of each lattice in the measure launch
+  const double* partials;
+  double* res;
+  int slot;               // 0 or 1 (initial / final configuration)
+  int D, N;
+  int scalar;
+};
+static __global__ void k_finalize(const FinArgs a) {
+  const int l = blockIdx.x;
+  const int b0 = a.blk_first[l], b1 = a.blk_first[l + 1];
+  __shared__ double sh[NRED][32];
+  double v[NRED] = {0, 0, 0, 0, 0, 0};
+  for (int b = b0 + (int)threadIdx.x; b < b1; b += 32)
+#pragma unroll
+    for (int k = 0; k < NRED; ++k) v[k] += a.partials[(size_t)b * NRED + k];
+#pragma unroll
+  for (int k = 0; k < NRED; ++k) sh[k][threadIdx.x] = v[k];
+  __syncwarp();
+  if (threadIdx.x == 0) {
+    double t[NRED];
+#pragma unroll
+    for (int k = 0; k < NRED; ++k) { t[k] = 0.0; for (int q = 0; q < 32; ++q) t[k] += sh[k][q]; }
+    const LatDev L = a.lats[l];
+    const double Vd = (double)L.V;
+    const double nplaq = Vd * (a.D * (a.D - 1) / 2);
+    const double Sg = (L.beta / a.N) * ((double)a.N * nplaq - t[0]);
+    const double SH = a.scalar ? (t[1] - 2.0 * L.kappa * t[2]) : 0.0;
+    const double kP = 0.5 * t[3], kpi = 0.5 * t[4];
+    double* o = a.res + ((size_t)l * 2 + a.slot) * NRES;
+    o[0] = kP + kpi + Sg + SH;
+    o[1] = Sg;
+    o[2] = SH;
+    o[3] = kP;
+    o[4] = kpi;
+    o[5] = t[0] / ((double)a.N * nplaq);
+    o[6] = a.scalar ? t[2] / (Vd * a.D) : 0.0;
+    o[7] = a.scalar ? t[5] / Vd : 0.0;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Metropolis (src/hmc/gauge_higgs_hmc.hpp:183-191, src/hmc/hmc.hpp:280-287): one
+// thread per lattice; dH from the two measure slots, ++traj, coin
+// uniform(key(0xE5 | 0xB2, traj)); NaN/Inf dH rejects (as in the reference,
+// where every comparison with NaN is false) and is counted.  Appends a record.
+// ---------------------------------------------------------------------------
+struct TrajRec { double dH; int accepted; int traj; double plaq, L_phi, L_link; };
+struct MetroArgs { LatDev* lats; const double* res; TrajRec* hist; int hist_cap; int nlat; int pure; };
+static __global__ void k_metropolis(const MetroArgs a) {
+  const int l = blockIdx.x * blockDim.x + threadIdx.x;
+  if (l >= a.nlat) return;
+  LatDev& L = a.lats[l];
+  const double* r0 = a.res + (size_t)l * 2 * NRES;
+  const double* r1 = r0 + NRES;
+  const double dH = r1[0] - r0[0];
+  L.traj += 1;
+  const double u = ghrng::uniform(L.seed, ghrng::key(a.pure ? 0xB2 : 0xE5, L.traj));
+  const bool finite = isfinite(dH);
+  const int acc = (dH <= 0.0) || (u < exp(-dH));
+  if (!finite) L.nonfinite += 1;
+  L.last_acc = acc;
+  L.accepted += acc;
+  if (a.hist && a.hist_cap > 0) {
+    TrajRec& h = a.hist[(size_t)l * a.hist_cap + (int)((L.traj - 1) % (unsigned long long)a.hist_cap)];
+    const double* ro = acc ? r1 : r0;
+    h.dH = dH;
+    h.accepted = acc;
+    h.traj = (int)L.traj;
+    h.plaq = ro[5];
+    h.L_phi = ro[7];
+    h.L_link = ro[6];
+  }
+}
+
+// Restore the saved configuration of lattices whose trajectory was rejected.
+struct RestoreArgs { const Work* work; const LatDev* lats; void* U; const void* Us; void* phi; const void* phis; int N; int d; };
+template <typename R>
+__global__ void __launch_bounds__(KBLOCK) k_restore(const RestoreArgs a) {
+  const Work w = a.work[blockIdx.x];
+  if ((int)threadIdx.x >= w.n) return;
+  const LatDev& L = a.lats[w.lat];
+  if (L.last_acc) return;
+  const int s = w.s0 + threadIdx.x;
+  typedef typename V2<R>::t V;
+  if (w.mu >= 0) {
+    const int NN = a.N * a.N;
+    const long long b = L.u_off + (long long)w.mu * NN * L.V + s;
+    for (int c = 0; c < NN; ++c) reinterpret_cast<V*>(a.U)[b + (long long)c * L.V] = reinterpret_cast<const V*>(a.Us)[b + (long long)c * L.V];
+  } else {
+    for (int k = 0; k < a.d; ++k) {
+      const long long i = L.f_off + (long long)k * L.V + s;
+      reinterpret_cast<V*>(a.phi)[i] = reinterpret_cast<const V*>(a.phis)[i];
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Counter-RNG field initialisation (bit-exact keys of the reference):
+//   hot start  U = expi(alg_to_mat(sigma * gauss(key(1, s, mu, a))))  src/core/fields.hpp:25-34
+//   momenta    P^a = gauss(key(stream, s, mu, a))                       src/core/fields.hpp:59-66
+//   vectors    re = sigma gauss(key(stream, s, 2k)), im = sigma gauss(key(stream, s, 2k+1)) or 0
+//                                                                       src/core/scalar_field.hpp:40-50
+//   refresh streams key(0xC3|0xA1, traj) and key(0xD4, traj)           src/hmc/gauge_higgs_hmc.hpp:167-173
+// ---------------------------------------------------------------------------
+struct InitArgs {
+  const Work* work;
+  const LatDev* lats;
+  void* U;
+  void* P;
+  void* vec;          // phi or pi
+  int what;           // 0 hot start, 1 momentum refresh (trajectory keys), 2 vector gaussian
+                      // 3 momentum with explicit stream, 4 cold links, 5 cold vector
+  int pure;           // pure gauge keys (0xA1) for what == 1
+  int real;
+  int d;
+  double sigma;
+  unsigned long long stream;
+};
+template <int N, typename R>
+__global__ void __launch_bounds__(KBLOCK) k_init(const InitArgs a) {
+  typedef typename Cmp<R>::t C;
+  const Work w = a.work[blockIdx.x];
+  if ((int)threadIdx.x >= w.n) return;
+  const LatDev L = a.lats[w.lat];
+  const int s = w.s0 + threadIdx.x;
+  constexpr int ng = N * N - 1;
+  if (w.mu >= 0) {
+    const int mu = w.mu;
+    if (a.what == 0 || a.what == 4) {
+      Mat<N, double> M;
+      if (a.what == 0) {
+        double v[ng];
+#pragma unroll
+        for (int g = 0; g < ng; ++g) v[g] = a.sigma * ghrng::gauss(L.seed, ghrng::key(1, s, mu, g));
+        M = expi<N>(alg_to_mat<N, double>(v));
+      } else {
+        set_ident(M);
+      }
+      st_link<N, double>((R*)a.U, L, mu, s, M);
+    } else if (a.what == 1 || a.what == 3) {
+      const unsigned long long st = (a.what == 1) ? ghrng::key(a.pure ? 0xA1 : 0xC3, L.traj) : a.stream;
+      R* P = (R*)a.P;
+      const long long pb = L.p_off + (long long)mu * ng * L.V + s;
+#pragma unroll
+      for (int g = 0; g < ng; ++g) P[pb + (long long)g * L.V] = (R)ghrng::gauss(L.seed, ghrng::key(st, s, mu, g));
+    }
+    return;
+  }
+  // site items: vectors (pi on refresh, phi on gaussian / cold start)
+  if (a.what == 1 && a.pure) return;
+  if (a.what == 1 || a.what == 2) {
+    const unsigned long long st = (a.what == 1) ? ghrng::key(0xD4, L.traj) : a.stream;
+    const double sg = (a.what == 1) ? 1.0 : a.sigma;
+    R* vec = (R*)a.vec;
+    for (int k = 0; k < a.d; ++k) {
+      const double re = sg * ghrng::gauss(L.seed, ghrng::key(st, s, 2 * k));
+      const double im = a.real ? 0.0 : sg * ghrng::gauss(L.seed, ghrng::key(st, s, 2 * k + 1));
+      stc<double>(vec, L.f_off + (long long)k * L.V + s, mk<double>(re, im));
+    }
+  } else if (a.what == 5) {
+    R* vec = (R*)a.vec;
+    for (int k = 0; k < a.d; ++k) stc<double>(vec, L.f_off + (long long)k * L.V + s, mk<double>(k == 0 ? a.sigma : 0.0, 0.0));
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Polyakov loop (src/measure/observables.hpp:17-34): one thread per site with
+// x_t = 0, product of the L_t links in direction t, FP64.
+// ---------------------------------------------------------------------------
+struct PolyArgs { const Work* work; const LatDev* lats; const void* U; int tdir; double* partials; };
+template <int D, int N, typename R>
+__global__ void __launch_bounds__(KBLOCK) k_polyakov(const PolyArgs a) {
+  const Work w = a.work[blockIdx.x];
+  double v = 0.0;
+  if ((int)threadIdx.x < w.n) {
+    const LatDev L = a.lats[w.lat];
+    const int s = w.s0 + threadIdx.x;
+    int x[D];
+    coords<D>(L, s, x);
+    if (x[a.tdir] == 0) {
+      const int t = a.tdir;
+      Mat<N, double> P = ld_link<N, double>((const R*)a.U, L, t, s);
+      int cur = s, xt = 0;
+      for (int k = 1; k < L.L[t]; ++k) {
+        cur = nfwd(L, cur, xt, t);
+        ++xt;
+        P = mm(P, ld_link<N, double>((const R*)a.U, L, t, cur));
+      }
+      for (int i = 0; i < N; ++i) v += P.e[i * N + i].re;
+    }
+  }
+  __shared__ double red[KBLOCK / 32];
+  v = warp_sum(v);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0.0;
+    for (int q = 0; q < KBLOCK / 32; ++q) t += red[q];
+    a.partials[blockIdx.x] = t;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Layout conversion between the reference's AoS host arrays (FP64) and the
+// device SoA planes (R).  kind: 0 links (N*N complex per (site,mu)),
+// 1 momenta (ng reals per (site,mu)), 2 vectors (d complex per site).
+// ---------------------------------------------------------------------------
+struct XferArgs { const LatDev* lats; int lat; int kind; int D; int ncomp; double* host_aos; void* dev; int to_dev; };
+template <typename R>
+__global__ void k_xfer(const XferArgs a) {
+  const LatDev L = a.lats[a.lat];
+  const long long per_site = (a.kind == 2) ? a.ncomp : (long long)a.D * a.ncomp;
+  const long long total = (long long)L.V * per_site;
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total; e += (long long)gridDim.x * blockDim.x) {
+    const int s = (int)(e / per_site);
+    const int r = (int)(e % per_site);
+    if (a.kind == 1) {
+      const long long di = L.p_off + (long long)r * L.V + s;   // r = mu*ng + g
+      R* P = (R*)a.dev;
+      if (a.to_dev) P[di] = (R)a.host_aos[e]; else a.host_aos[e] = (double)P[di];
+    } else {
+      const long long di = ((a.kind == 0) ? L.u_off : L.f_off) + (long long)r * L.V + s;  // r = mu*NN + c or k
+      if (a.to_dev) stc<double>((R*)a.dev, di, mk<double>(a.host_aos[2 * e], a.host_aos[2 * e + 1]));
+      else { const cx<double> z = ldc_rw<double>((const R*)a.dev, di); a.host_aos[2 * e] = z.re; a.host_aos[2 * e + 1] = z.im; }
+    }
+  }
+}
+
+}  // namespace ghk

@@ -1,0 +1,339 @@
+// gh_math.cuh -- register-resident SU(N) algebra for the MD kernels.
+//
+// Conventions are the reference's (docs/conventions.md): Hermitian generators
+// T^a = Lambda^a / 2 in generalised Gell-Mann order (symmetric pairs,
+// antisymmetric pairs, diagonal; src/group/algebra.hpp:23-49), Tr T^aT^b = d/2.
+// Nothing here materialises T^a: projections Im Tr(T^a M), 2 Tr(T^a M) and the
+// map v -> sum_a v_a T^a are written out entry by entry from the sparse
+// structure of the generators, which is what makes them cheap in registers.
+#pragma once
+#include <stdint.h>
+#include <math.h>
+
+#if defined(__CUDACC__)
+#define GH_HD __host__ __device__ __forceinline__
+#define GH_D __device__ __forceinline__
+#else
+#define GH_HD inline
+#define GH_D inline
+#endif
+
+namespace ghm {
+
+template <typename T> struct cx { T re, im; };
+
+template <typename T> GH_HD cx<T> mk(T r, T i) { cx<T> z; z.re = r; z.im = i; return z; }
+template <typename T> GH_HD cx<T> zero() { return mk<T>(T(0), T(0)); }
+template <typename T> GH_HD cx<T> add(cx<T> a, cx<T> b) { return mk<T>(a.re + b.re, a.im + b.im); }
+template <typename T> GH_HD cx<T> sub(cx<T> a, cx<T> b) { return mk<T>(a.re - b.re, a.im - b.im); }
+template <typename T> GH_HD cx<T> mul(cx<T> a, cx<T> b) { return mk<T>(a.re * b.re - a.im * b.im, a.re * b.im + a.im * b.re); }
+// a * conj(b)
+template <typename T> GH_HD cx<T> mulc(cx<T> a, cx<T> b) { return mk<T>(a.re * b.re + a.im * b.im, a.im * b.re - a.re * b.im); }
+// conj(a) * b
+template <typename T> GH_HD cx<T> cmul(cx<T> a, cx<T> b) { return mk<T>(a.re * b.re + a.im * b.im, a.re * b.im - a.im * b.re); }
+// conj(a) * conj(b)
+template <typename T> GH_HD cx<T> cmulc(cx<T> a, cx<T> b) { return mk<T>(a.re * b.re - a.im * b.im, -(a.re * b.im + a.im * b.re)); }
+template <typename T> GH_HD cx<T> conj(cx<T> a) { return mk<T>(a.re, -a.im); }
+template <typename T> GH_HD cx<T> scale(cx<T> a, T s) { return mk<T>(a.re * s, a.im * s); }
+template <typename T> GH_HD T norm2(cx<T> a) { return a.re * a.re + a.im * a.im; }
+template <typename T, typename S> GH_HD cx<T> cvt(cx<S> a) { return mk<T>((T)a.re, (T)a.im); }
+
+template <int N, typename T> struct Mat { cx<T> e[N * N]; };
+
+template <int N, typename T> GH_HD void set_zero(Mat<N, T>& A) {
+#pragma unroll
+  for (int i = 0; i < N * N; ++i) A.e[i] = zero<T>();
+}
+template <int N, typename T> GH_HD void set_ident(Mat<N, T>& A) {
+#pragma unroll
+  for (int i = 0; i < N; ++i)
+#pragma unroll
+    for (int j = 0; j < N; ++j) A.e[i * N + j] = mk<T>(i == j ? T(1) : T(0), T(0));
+}
+template <int N, typename T> GH_HD void acc(Mat<N, T>& A, const Mat<N, T>& B) {
+#pragma unroll
+  for (int i = 0; i < N * N; ++i) A.e[i] = add(A.e[i], B.e[i]);
+}
+
+// C = A B ; C = A B^dag ; C = A^dag B ; C = A^dag B^dag   (sum over k in order 0..N-1)
+template <int N, typename T> GH_HD Mat<N, T> mm(const Mat<N, T>& A, const Mat<N, T>& B) {
+  Mat<N, T> C;
+#pragma unroll
+  for (int i = 0; i < N; ++i)
+#pragma unroll
+    for (int j = 0; j < N; ++j) {
+      cx<T> s = mul(A.e[i * N], B.e[j]);
+#pragma unroll
+      for (int k = 1; k < N; ++k) s = add(s, mul(A.e[i * N + k], B.e[k * N + j]));
+      C.e[i * N + j] = s;
+    }
+  return C;
+}
+template <int N, typename T> GH_HD Mat<N, T> mm_nd(const Mat<N, T>& A, const Mat<N, T>& B) {
+  Mat<N, T> C;
+#pragma unroll
+  for (int i = 0; i < N; ++i)
+#pragma unroll
+    for (int j = 0; j < N; ++j) {
+      cx<T> s = mulc(A.e[i * N], B.e[j * N]);
+#pragma unroll
+      for (int k = 1; k < N; ++k) s = add(s, mulc(A.e[i * N + k], B.e[j * N + k]));
+      C.e[i * N + j] = s;
+    }
+  return C;
+}
+template <int N, typename T> GH_HD Mat<N, T> mm_dn(const Mat<N, T>& A, const Mat<N, T>& B) {
+  Mat<N, T> C;
+#pragma unroll
+  for (int i = 0; i < N; ++i)
+#pragma unroll
+    for (int j = 0; j < N; ++j) {
+      cx<T> s = cmul(A.e[i], B.e[j]);
+#pragma unroll
+      for (int k = 1; k < N; ++k) s = add(s, cmul(A.e[k * N + i], B.e[k * N + j]));
+      C.e[i * N + j] = s;
+    }
+  return C;
+}
+template <int N, typename T> GH_HD Mat<N, T> mm_dd(const Mat<N, T>& A, const Mat<N, T>& B) {
+  Mat<N, T> C;
+#pragma unroll
+  for (int i = 0; i < N; ++i)
+#pragma unroll
+    for (int j = 0; j < N; ++j) {
+      cx<T> s = cmulc(A.e[i], B.e[j * N]);
+#pragma unroll
+      for (int k = 1; k < N; ++k) s = add(s, cmulc(A.e[k * N + i], B.e[j * N + k]));
+      C.e[i * N + j] = s;
+    }
+  return C;
+}
+// Re Tr(A B^dag) = sum_ij Re(A_ij conj(B_ij))
+template <int N, typename T> GH_HD T retr_nd(const Mat<N, T>& A, const Mat<N, T>& B) {
+  T s = T(0);
+#pragma unroll
+  for (int i = 0; i < N * N; ++i) s += A.e[i].re * B.e[i].re + A.e[i].im * B.e[i].im;
+  return s;
+}
+template <int N, typename T> GH_HD T fnorm2(const Mat<N, T>& A) {
+  T s = T(0);
+#pragma unroll
+  for (int i = 0; i < N * N; ++i) s += norm2(A.e[i]);
+  return s;
+}
+
+// ---------------------------------------------------------------------------
+// Generator maps (generalised Gell-Mann, T = Lambda/2).
+// ---------------------------------------------------------------------------
+template <int N> GH_HD constexpr int ngen() { return N * N - 1; }
+template <int N> GH_HD constexpr int npair() { return N * (N - 1) / 2; }
+
+// diagonal generator l (1..N-1): T_jj = c_l/2 (j<l), T_ll = -l c_l/2, c_l = sqrt(2/(l(l+1)))
+GH_HD double diag_c(int l) {
+  return (l == 1) ? 1.0 : (l == 2) ? 0.57735026918962573 : (l == 3) ? 0.40824829046386302 : sqrt(2.0 / (double)(l * (l + 1)));
+}
+
+// F_a = Im Tr(T^a M)   (the component projection of src/action/gauge_wilson.hpp:80-81)
+template <int N, typename T> GH_HD void im_tr_proj(const Mat<N, T>& M, T* F) {
+  int a = 0;
+#pragma unroll
+  for (int j = 0; j < N; ++j)
+#pragma unroll
+    for (int k = j + 1; k < N; ++k) F[a++] = T(0.5) * (M.e[k * N + j].im + M.e[j * N + k].im);
+#pragma unroll
+  for (int j = 0; j < N; ++j)
+#pragma unroll
+    for (int k = j + 1; k < N; ++k) F[a++] = T(0.5) * (M.e[j * N + k].re - M.e[k * N + j].re);
+#pragma unroll
+  for (int l = 1; l < N; ++l) {
+    T s = T(0);
+#pragma unroll
+    for (int j = 0; j < l; ++j) s += M.e[j * N + j].im;
+    F[a++] = T(0.5 * diag_c(l)) * (s - T(l) * M.e[l * N + l].im);
+  }
+}
+// z_a = 2 Tr(T^a M) (complex); the inverse of alg_to_mat on traceless matrices
+template <int N, typename T> GH_HD void tr2_proj(const Mat<N, T>& M, cx<T>* z) {
+  int a = 0;
+#pragma unroll
+  for (int j = 0; j < N; ++j)
+#pragma unroll
+    for (int k = j + 1; k < N; ++k) z[a++] = add(M.e[k * N + j], M.e[j * N + k]);
+#pragma unroll
+  for (int j = 0; j < N; ++j)
+#pragma unroll
+    for (int k = j + 1; k < N; ++k) {
+      const cx<T> d = sub(M.e[j * N + k], M.e[k * N + j]);   // -i M_kj + i M_jk = i (M_jk - M_kj)
+      z[a++] = mk<T>(-d.im, d.re);
+    }
+#pragma unroll
+  for (int l = 1; l < N; ++l) {
+    cx<T> s = zero<T>();
+#pragma unroll
+    for (int j = 0; j < l; ++j) s = add(s, M.e[j * N + j]);
+    s = sub(s, scale(M.e[l * N + l], T(l)));
+    z[a++] = scale(s, T(diag_c(l)));
+  }
+}
+// M = sum_a v_a T^a for real v (src/group/algebra.hpp:59-71)
+template <int N, typename T> GH_HD Mat<N, T> alg_to_mat(const T* v) {
+  Mat<N, T> M;
+  set_zero(M);
+  int a = 0;
+  const int np = npair<N>();
+#pragma unroll
+  for (int j = 0; j < N; ++j)
+#pragma unroll
+    for (int k = j + 1; k < N; ++k, ++a) {
+      const T s = T(0.5) * v[a], t = T(0.5) * v[a + np];
+      M.e[j * N + k] = mk<T>(s, -t);
+      M.e[k * N + j] = mk<T>(s, t);
+    }
+  a += np;
+#pragma unroll
+  for (int l = 1; l < N; ++l, ++a) {
+    const T h = T(0.5 * diag_c(l)) * v[a];
+#pragma unroll
+    for (int j = 0; j < l; ++j) M.e[j * N + j].re += h;
+    M.e[l * N + l].re -= T(l) * h;
+  }
+  return M;
+}
+// M = sum_a z_a T^a for complex z
+template <int N, typename T> GH_HD Mat<N, T> alg_to_mat_c(const cx<T>* z) {
+  Mat<N, T> M;
+  set_zero(M);
+  int a = 0;
+  const int np = npair<N>();
+#pragma unroll
+  for (int j = 0; j < N; ++j)
+#pragma unroll
+    for (int k = j + 1; k < N; ++k, ++a) {
+      const cx<T> s = scale(z[a], T(0.5)), t = scale(z[a + np], T(0.5));
+      // T_sym: 1/2 at (j,k),(k,j); T_anti: -i/2 at (j,k), +i/2 at (k,j)
+      M.e[j * N + k] = add(s, mk<T>(t.im, -t.re));
+      M.e[k * N + j] = add(s, mk<T>(-t.im, t.re));
+    }
+  a += np;
+#pragma unroll
+  for (int l = 1; l < N; ++l, ++a) {
+    const cx<T> h = scale(z[a], T(0.5 * diag_c(l)));
+#pragma unroll
+    for (int j = 0; j < l; ++j) M.e[j * N + j] = add(M.e[j * N + j], h);
+    M.e[l * N + l] = sub(M.e[l * N + l], scale(h, T(l)));
+  }
+  return M;
+}
+
+// ---------------------------------------------------------------------------
+// exp(iH), H Hermitian traceless, in FP64 (src/group/sun.hpp:11-45).
+// General N: scaling and squaring to ||A||_F <= 1/2, then the Taylor series,
+// stopped once a term falls below 1e-18 (the reference always sums 18 terms;
+// the terms it adds past that point are below FP64 resolution).
+// SU(2): the closed form cos r + i sin(r)/r H.
+// ---------------------------------------------------------------------------
+template <int N> GH_HD Mat<N, double> expi(const Mat<N, double>& H) {
+  const double nrm = sqrt(fnorm2(H));
+  int s = 0;
+  double scaled = nrm;
+  while (scaled > 0.5) { scaled *= 0.5; ++s; }
+  const double inv2s = ldexp(1.0, -s);
+  Mat<N, double> A, term, res;
+#pragma unroll
+  for (int i = 0; i < N * N; ++i) A.e[i] = mk<double>(-H.e[i].im * inv2s, H.e[i].re * inv2s);
+  set_ident(term);
+  set_ident(res);
+  for (int k = 1; k <= 18; ++k) {
+    term = mm(term, A);
+    const double ik = 1.0 / k;
+#pragma unroll
+    for (int i = 0; i < N * N; ++i) term.e[i] = scale(term.e[i], ik);
+    acc(res, term);
+    if (fnorm2(term) < 1e-36) break;
+  }
+  for (int i = 0; i < s; ++i) res = mm(res, res);
+  return res;
+}
+template <> GH_HD Mat<2, double> expi<2>(const Mat<2, double>& H) {
+  // r^2 = Tr(H^2)/2
+  double trh2 = 0.0;
+#pragma unroll
+  for (int i = 0; i < 2; ++i)
+#pragma unroll
+    for (int k = 0; k < 2; ++k) trh2 += mul(H.e[i * 2 + k], H.e[k * 2 + i]).re;
+  const double r2 = 0.5 * trh2;
+  const double r = sqrt(r2 > 0.0 ? r2 : 0.0);
+  double c, sinc;
+  if (r < 1e-8) { c = 1.0 - 0.5 * r2; sinc = 1.0 - r2 / 6.0; }
+  else { double sn; sincos(r, &sn, &c); sinc = sn / r; }
+  Mat<2, double> U;
+#pragma unroll
+  for (int i = 0; i < 4; ++i) U.e[i] = mk<double>(-sinc * H.e[i].im, sinc * H.e[i].re);
+  U.e[0].re += c;
+  U.e[3].re += c;
+  return U;
+}
+
+// Determinant (N <= 4), Gaussian elimination without pivoting for N=4 falls back
+// to cofactors; N=2,3 closed forms.
+template <int N, typename T> GH_HD cx<T> det(const Mat<N, T>& U) {
+  if (N == 2) return sub(mul(U.e[0], U.e[3]), mul(U.e[1], U.e[2]));
+  if (N == 3) {
+    const cx<T> c0 = sub(mul(U.e[4], U.e[8]), mul(U.e[5], U.e[7]));
+    const cx<T> c1 = sub(mul(U.e[5], U.e[6]), mul(U.e[3], U.e[8]));
+    const cx<T> c2 = sub(mul(U.e[3], U.e[7]), mul(U.e[4], U.e[6]));
+    return add(add(mul(U.e[0], c0), mul(U.e[1], c1)), mul(U.e[2], c2));
+  }
+  // generic: elimination with partial pivoting on a copy
+  Mat<N, T> m = U;
+  cx<T> d = mk<T>(T(1), T(0));
+  for (int col = 0; col < N; ++col) {
+    int piv = col;
+    T best = norm2(m.e[col * N + col]);
+    for (int r = col + 1; r < N; ++r) { T v = norm2(m.e[r * N + col]); if (v > best) { best = v; piv = r; } }
+    if (best == T(0)) return zero<T>();
+    if (piv != col) {
+      for (int j = 0; j < N; ++j) { cx<T> t = m.e[piv * N + j]; m.e[piv * N + j] = m.e[col * N + j]; m.e[col * N + j] = t; }
+      d = mk<T>(-d.re, -d.im);
+    }
+    d = mul(d, m.e[col * N + col]);
+    const T in2 = T(1) / norm2(m.e[col * N + col]);
+    const cx<T> inv = scale(conj(m.e[col * N + col]), in2);
+    for (int r = col + 1; r < N; ++r) {
+      const cx<T> f = mul(m.e[r * N + col], inv);
+      for (int j = col; j < N; ++j) m.e[r * N + j] = sub(m.e[r * N + j], mul(f, m.e[col * N + j]));
+    }
+  }
+  return d;
+}
+
+// Modified Gram-Schmidt on rows, then det phase removed from row 0
+// (src/group/sun.hpp:48-71).
+template <int N, typename T> GH_HD void reunitarize(Mat<N, T>& U) {
+#pragma unroll
+  for (int i = 0; i < N; ++i) {
+#pragma unroll
+    for (int k = 0; k < i; ++k) {
+      cx<T> p = zero<T>();
+#pragma unroll
+      for (int j = 0; j < N; ++j) p = add(p, cmul(U.e[k * N + j], U.e[i * N + j]));
+#pragma unroll
+      for (int j = 0; j < N; ++j) U.e[i * N + j] = sub(U.e[i * N + j], mul(p, U.e[k * N + j]));
+    }
+    T n = T(0);
+#pragma unroll
+    for (int j = 0; j < N; ++j) n += norm2(U.e[i * N + j]);
+    const T inv = T(1) / sqrt(n);
+#pragma unroll
+    for (int j = 0; j < N; ++j) U.e[i * N + j] = scale(U.e[i * N + j], inv);
+  }
+  const cx<T> d = det<N, T>(U);
+  const T ad = sqrt(norm2(d));
+  if (ad > T(0)) {
+    const cx<T> ph = mk<T>(d.re / ad, -d.im / ad);   // conj(d/|d|)
+#pragma unroll
+    for (int j = 0; j < N; ++j) U.e[j] = mul(U.e[j], ph);
+  }
+}
+
+}  // namespace ghm

@@ -1,0 +1,202 @@
+/* gauge_higgs_b200.h -- C ABI of the B200 molecular-dynamics engine for SU(N)
+ * gauge + arbitrary-irrep Higgs Hybrid Monte Carlo.
+ *
+ * The reference (hlammiv/gauge_higgs) has no C ABI: its hot path is a C++
+ * template / virtual interface.  Each entry point below names the reference
+ * interface it replaces (paths relative to that project's root).  A host driver
+ * keeps its compile-time NDIM/NCOL and its Representation objects and hands the
+ * per-step work to these calls.
+ *
+ * Conventions
+ *  - Host arrays use the reference's layouts (array of structures), FP64:
+ *      links    U   [site][mu][i][j] complex   (src/core/fields.hpp:12-20)
+ *      momenta  P   [site][mu][a]    double    (src/core/fields.hpp:46-57)
+ *      vectors  phi [site][k]        complex   (src/core/scalar_field.hpp:15)
+ *    complex = two doubles (re, im); site index mixed radix, direction 0 fastest
+ *    (src/core/geometry.hpp:20-38).
+ *  - Every call returns GH_OK (0) or a negative GH_ERR_* code; no exception
+ *    crosses the ABI.  gh_last_error(ctx) gives the message (ctx may be NULL
+ *    for errors of gh_ctx_create).  The reference throws std::runtime_error
+ *    (e.g. src/rep/rep_general.hpp:58-69) and its driver exits 1
+ *    (src/hmc_higgs.cpp:57-59).
+ *  - A context owns all device memory and one CUDA stream; calls on one context
+ *    are stream ordered and not thread safe; distinct contexts may be used from
+ *    distinct threads.  Host pointers are only borrowed for the duration of a
+ *    call; calls that return host data synchronise the stream.
+ *  - A context may hold several independent lattices ("batch") of one (D, N,
+ *    representation) with their own extents, couplings, seeds and trajectory
+ *    counters.  Per-lattice calls take `lat` (0-based); `lat = -1` means all.
+ */
+#ifndef GAUGE_HIGGS_B200_H
+#define GAUGE_HIGGS_B200_H
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define GH_OK 0
+#define GH_ERR_ARG -1
+#define GH_ERR_CUDA -2
+#define GH_ERR_REP -3
+#define GH_ERR_STATE -4
+#define GH_ERR_NONFINITE -5
+#define GH_ERR_UNSUPPORTED -6
+
+enum { GH_REP_NONE = 0, GH_REP_FUND = 1, GH_REP_ADJ = 2, GH_REP_GENERAL = 3 };
+enum { GH_PREC_FP64 = 0, GH_PREC_FP32_MD = 1 };
+enum { GH_LEAPFROG = 0, GH_OMELYAN = 1 };
+
+/* Representation R of the scalar.  Replaces the Representation<N> object
+ * (src/rep/representation.hpp:12-32).  GENERAL carries the host-built tables of
+ * GeneralRep<N> (src/rep/rep_general.hpp:36-42): T^a_R = T[a][i][j] and the
+ * irrep basis W[l][t] of V^{x n} (Wflat).  For FUND and ADJ the tables are
+ * implied (T, W may be NULL). */
+typedef struct {
+  int kind;          /* GH_REP_* */
+  int d;             /* representation dimension d(R) */
+  int real;          /* scalar carries d real dof (heatbath imaginary parts zero) */
+  int n_boxes;       /* Young boxes n (GENERAL) */
+  long dimT;         /* N^n (GENERAL) */
+  const double* T;   /* [N*N-1][d][d] complex (GENERAL, required) */
+  const double* W;   /* [d][dimT] complex (GENERAL, required) */
+} gh_rep_desc;
+
+/* Per-lattice measurement: H and its parts (src/hmc/gauge_higgs_hmc.hpp:105-110),
+ * avg_plaquette (src/action/gauge_wilson.hpp:50-65), link_energy and
+ * higgs_length (src/action/scalar_higgs.hpp:132-154). */
+typedef struct {
+  double H, S_g, S_H, kin_P, kin_pi, plaquette, L_link, L_phi;
+} gh_obs;
+
+/* One trajectory of one lattice: dH, accept, and the driver's measurements
+ * after accept/reject (src/hmc_higgs.cpp:80-87). */
+typedef struct {
+  double dH;
+  int accepted;
+  int traj;
+  double plaquette, L_phi, L_link;
+} gh_traj_record;
+
+typedef struct gh_ctx gh_ctx;
+
+/* ---- context ------------------------------------------------------------
+ * Replaces construction of GaugeHiggsHMC<D,N>(extents, rep, seed)
+ * (src/hmc/gauge_higgs_hmc.hpp:45-50) and GaugeHMC<D,N>(extents, seed)
+ * (src/hmc/hmc.hpp:226-227; rep == NULL or kind GH_REP_NONE selects it).
+ * L: n_lat * D extents; seeds: n_lat Rng seeds (src/core/rng.hpp:19-22). */
+int gh_ctx_create(int D, int N, int n_lat, const int* L, const gh_rep_desc* rep, int precision,
+                  const uint64_t* seeds, gh_ctx** out);
+int gh_ctx_destroy(gh_ctx* ctx);
+const char* gh_last_error(const gh_ctx* ctx);
+/* Launch on an external CUDA stream (cudaStream_t passed as void*); NULL restores the own stream. */
+int gh_set_stream(gh_ctx* ctx, void* stream);
+int gh_sync(gh_ctx* ctx);
+int gh_info(const gh_ctx* ctx, int* D, int* N, int* n_lat, int* d, int* rep_kind, int* precision);
+/* Device bytes held by the context (fields, scratch, tables). */
+int gh_device_bytes(const gh_ctx* ctx, uint64_t* bytes);
+
+/* ---- couplings / integrator (the public members beta, kappa, lambda, tau,
+ * nmd, integ, traj_count of GaugeHiggsHMC, src/hmc/gauge_higgs_hmc.hpp:24-42) */
+int gh_set_couplings(gh_ctx* ctx, int lat, double beta, double kappa, double lambda);
+int gh_get_couplings(gh_ctx* ctx, int lat, double* beta, double* kappa, double* lambda);
+int gh_set_integrator(gh_ctx* ctx, int integ, int nmd, double tau);
+int gh_set_traj_count(gh_ctx* ctx, int lat, uint64_t traj_count, uint64_t accept_count);
+int gh_get_traj_count(gh_ctx* ctx, int lat, uint64_t* traj_count, uint64_t* accept_count,
+                      uint64_t* nonfinite_count);
+
+/* ---- fields: AoS host <-> device (the std::vector members U.u, P.p, phi.data,
+ * pi.data of src/hmc/gauge_higgs_hmc.hpp:18-20) ---- */
+int gh_set_links(gh_ctx* ctx, int lat, const double* U);
+int gh_get_links(gh_ctx* ctx, int lat, double* U);
+int gh_set_mom(gh_ctx* ctx, int lat, const double* P);
+int gh_get_mom(gh_ctx* ctx, int lat, double* P);
+int gh_set_phi(gh_ctx* ctx, int lat, const double* phi);
+int gh_get_phi(gh_ctx* ctx, int lat, double* phi);
+int gh_set_pi(gh_ctx* ctx, int lat, const double* pi);
+int gh_get_pi(gh_ctx* ctx, int lat, double* pi);
+
+/* ---- initialisation with the reference's counter-RNG keys ----
+ * gh_hot_start:      GaugeField::hot(rng, sigma)            src/core/fields.hpp:25-34
+ * gh_cold_start:     GaugeField::cold()                     src/core/fields.hpp:23
+ * gh_phi_gaussian:   CVecField::gaussian(rng, stream, rep.real, sigma)  src/core/scalar_field.hpp:40-50
+ * gh_phi_cold:       CVecField::cold(c)                     src/core/scalar_field.hpp:34-37
+ * gh_mom_refresh:    LinkMom::refresh(rng, stream)          src/core/fields.hpp:59-66
+ * gh_refresh_momenta: GaugeHiggsHMC::refresh_momenta (keys 0xC3 / 0xD4 at traj_count)
+ *                    src/hmc/gauge_higgs_hmc.hpp:167-173, GaugeHMC 0xA1 src/hmc/hmc.hpp:271-272
+ * All act on every lattice with that lattice's seed. */
+int gh_hot_start(gh_ctx* ctx, double sigma);
+int gh_cold_start(gh_ctx* ctx);
+int gh_phi_gaussian(gh_ctx* ctx, uint64_t stream, double sigma);
+int gh_phi_cold(gh_ctx* ctx, double c);
+int gh_mom_refresh(gh_ctx* ctx, uint64_t stream);
+int gh_refresh_momenta(gh_ctx* ctx);
+
+/* ---- forces (FP64 host output, AoS; one lattice) ----
+ * gh_gauge_force:       add_gauge_force onto zero           src/action/gauge_wilson.hpp:70-83
+ * gh_matter_link_force: add_matter_link_force onto zero     src/action/scalar_higgs.hpp:113-128
+ *                       (uses Representation::hop_link_g, src/rep/representation.hpp:36-46)
+ * gh_scalar_force:      scalar_force                        src/action/scalar_higgs.hpp:71-108
+ *                       (uses Representation::rotate / rotate_dag, :28-32) */
+int gh_gauge_force(gh_ctx* ctx, int lat, double* F);
+int gh_matter_link_force(gh_ctx* ctx, int lat, double* F);
+int gh_scalar_force(gh_ctx* ctx, int lat, double* Fphi);
+
+/* ---- integrator steps (all lattices) ----
+ * gh_kick:      GaugeHiggsHMC::kick(eps) / GaugeHMC::kick   src/hmc/gauge_higgs_hmc.hpp:112-134, src/hmc/hmc.hpp:35-41
+ * gh_drift:     ::drift(eps)                                 src/hmc/gauge_higgs_hmc.hpp:136-147, src/hmc/hmc.hpp:44-52
+ * gh_md_evolve: ::md_evolve() with the set integrator        src/hmc/gauge_higgs_hmc.hpp:149-165
+ * gh_reunitarize: GaugeField::reunitarize_all()             src/core/fields.hpp:36 */
+int gh_kick(gh_ctx* ctx, double eps);
+int gh_drift(gh_ctx* ctx, double eps);
+int gh_md_evolve(gh_ctx* ctx);
+int gh_reunitarize(gh_ctx* ctx);
+
+/* ---- measurements (one lattice, or lat = -1 with n_lat entries) ----
+ * gh_measure: hamiltonian() and its parts, avg_plaquette, link_energy, higgs_length.
+ * gh_polyakov: polyakov_loop(U, tdir)                       src/measure/observables.hpp:17-34 */
+int gh_measure(gh_ctx* ctx, int lat, gh_obs* out);
+int gh_polyakov(gh_ctx* ctx, int lat, int tdir, double* out);
+
+/* ---- trajectories ----
+ * gh_trajectory: GaugeHiggsHMC::trajectory() / GaugeHMC::trajectory() on every
+ * lattice (src/hmc/gauge_higgs_hmc.hpp:175-192, src/hmc/hmc.hpp:270-288):
+ * refresh, save, H_i, md_evolve, reunitarize (FP64 mode), H_f, Metropolis,
+ * restore on reject -- entirely on the device (captured once as a CUDA graph).
+ * dH, accepted: n_lat entries each (may be NULL).  NaN/Inf dH is rejected, as
+ * in the reference, and counted (gh_get_traj_count). */
+int gh_trajectory(gh_ctx* ctx, double* dH, int* accepted);
+/* ntraj trajectories back to back without host synchronisation in between;
+ * records: ntraj * n_lat entries [t][lat] (may be NULL). */
+int gh_run_trajectories(gh_ctx* ctx, int ntraj, gh_traj_record* records);
+/* Host-resident fields (single lattice): upload U and phi, run one trajectory,
+ * download U, phi and the record.  The drop-in for a driver that keeps the
+ * fields in host memory like the reference's GaugeField / CVecField. */
+int gh_trajectory_host(gh_ctx* ctx, double* U, double* phi, gh_traj_record* rec);
+/* Use (1, default) or bypass (0) the captured trajectory graph. */
+int gh_use_graph(gh_ctx* ctx, int enable);
+
+/* ---- replica tempering in kappa across the lattices of a batch ----
+ * The mechanism of ReplicaTempering::step / attempt_swap (src/hmc/replica_tempering.hpp:157-205)
+ * with kappa as the tempered coupling: after every trajectory, adjacent-kappa
+ * pairs of lattices with equal extents propose a configuration exchange with
+ * Delta = (kappa_i - kappa_j)(B_i - B_j), B = sum_{x,mu} 2 Re phi_x^dag D(U) phi_{x+mu},
+ * coin uniform(key(0x57A9, ++counter)) on swap_seed; even pass then odd pass.
+ * The exchange swaps the coupling labels on the device (equivalent to swapping
+ * U and phi).  mode 0 disables. */
+int gh_temper_enable(gh_ctx* ctx, int mode, uint64_t swap_seed);
+/* attempts/accepts: per adjacent pair in ladder order (n_lat - 1 entries);
+ * kappa_of_lat: current kappa of each lattice. */
+int gh_temper_stats(gh_ctx* ctx, uint64_t* attempts, uint64_t* accepts, double* kappa_of_lat);
+
+/* ---- general irreps: host-side construction of the GeneralRep tables ----
+ * The Young-symmetriser basis of src/rep/rep_general.hpp:54-84,338-411, so a
+ * driver without the reference headers can still form gh_rep_desc.
+ * rows: Young diagram row lengths. */
+int gh_rep_general_info(int N, const int* rows, int nrows, int* d, int* n_boxes, long* dimT);
+int gh_rep_general_build(int N, const int* rows, int nrows, double* T, double* W);
+
+#ifdef __cplusplus
+}
+#endif
+#endif
