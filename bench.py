@@ -1,0 +1,377 @@
+#!/usr/bin/env python
+"""Headline benchmark: SU(3) + fundamental-Higgs HMC on a 16^4 lattice,
+trajectories per second, FP32-MD (FP64 Hamiltonian) against the FP64 path on
+the same GPU, with the dominant kernel's roofline.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Workload (beta=5.7, kappa=0.10, lambda=0.5, Omelyan nmd=16, tau=1, hot start
+sigma=0.8 from Rng seed 1+rank, phi Gaussian sigma=0.3 on stream 12345): one
+step = one complete HMC trajectory (momentum heatbath, H_i, 16 Omelyan steps,
+H_f, Metropolis, restore on reject).  Inputs are synthetic (the reference's own
+counter RNG); there is no dataset.  The L2 cache (126 MB) is flushed between
+trajectories by writing a 256 MB buffer on the same stream, inside the timed
+region.  Multi-GPU: one independent replica lattice per rank (the single
+lattice does not shard), value = trajectories of all ranks / max rank time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WL = dict(D=4, N=3, L=[16, 16, 16, 16], spec="fund", beta=5.7, kappa=0.10, lam=0.5, nmd=16, tau=1.0,
+          integ="omelyan", hot_sigma=0.8, phi_sigma=0.3)
+WORKLOAD = ("SU(3) + fundamental Higgs, 4D 16^4 (65536 sites), beta=5.7 kappa=0.10 lambda=0.5, "
+            "Omelyan 2MN nmd=16 tau=1.0, hot start")
+METRIC = "SU(3)+Higgs 16^4 trajectories/s, FP32-MD vs FP64 GPU at equal obs; % HBM peak"
+# algorithmic bytes per site and launch (each field read / written once), SU(3) fundamental:
+#   kick  = U 576 + phi 48 + P read+write 512 + pi read+write 96 = 1232 B (FP64), half in FP32
+#   drift = P 256 + U read+write 1152 + pi 48 + phi read+write 96 = 1552 B (FP64), half in FP32
+ALG_BYTES = {"kick": {"fp64": 1232, "fp32": 616}, "drift": {"fp64": 1552, "fp32": 776}}
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class Dist:
+    def __init__(self):
+        self.world = int(os.environ.get("WORLD_SIZE", "1"))
+        self.rank = int(os.environ.get("RANK", "0"))
+        self.local = int(os.environ.get("LOCAL_RANK", "0"))
+        self.pg = None
+
+    def init(self, backend):
+        if self.world > 1:
+            import datetime
+            import torch.distributed as dist
+            dist.init_process_group(backend, timeout=datetime.timedelta(seconds=120))
+            self.pg = dist
+
+    def barrier(self):
+        if self.pg:
+            self.pg.barrier()
+
+    def max(self, x):
+        if not self.pg:
+            return x
+        import torch
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        self.pg.all_reduce(t, op=self.pg.ReduceOp.MAX)
+        return float(t.item())
+
+    def close(self):
+        if self.pg:
+            self.pg.destroy_process_group()
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during a timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.idx = gpu_index
+        self.p = None
+
+    def start(self):
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(self.idx), f"--query-gpu={self.Q}",
+                                       "--format=csv,noheader,nounits", "-lms", "100"], stdout=self.f,
+                                      stderr=subprocess.DEVNULL)
+        except Exception:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return None
+        self.p.terminate()
+        try:
+            self.p.wait(timeout=5)
+        except Exception:
+            self.p.kill()
+        self.f.flush()
+        rows = [r.split(",") for r in open(self.f.name).read().strip().splitlines() if r.strip()]
+        os.unlink(self.f.name)
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            r = [x.strip() for x in r]
+            if len(r) < 9:
+                continue
+            try:
+                sm.append(float(r[1]))
+                mx = float(r[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, r[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def launches_per_traj(nmd, prec):
+    # refresh 1 + (measure + finalize) x 2 + kicks (2 nmd + 1) + drifts 2 nmd
+    # + end-of-trajectory reunitarisation (FP64 mode only) + Metropolis 1 + restore 1
+    return 1 + 4 + (2 * nmd + 1) + 2 * nmd + (1 if prec == "fp64" else 0) + 2
+
+
+def run_ours(a, dist):
+    import torch
+    torch.cuda.set_device(dist.local)
+    dist.init("nccl")
+    import gauge_higgs_b200 as gh
+
+    # a dedicated stream: the engine captures its trajectory as a CUDA graph, which the
+    # legacy default stream cannot host; torch work (the L2 flush) goes to the same stream
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+
+    def make(prec):
+        h = gh.GaugeHiggsHMC(WL["L"], gh.FundamentalRep(WL["N"]), seed=1 + dist.rank, precision=prec,
+                             beta=WL["beta"], kappa=WL["kappa"], lam=WL["lam"], nmd=WL["nmd"], tau=WL["tau"],
+                             integ=WL["integ"])
+        h.set_stream(stream.cuda_stream)
+        h.hot(WL["hot_sigma"])
+        h.phi_gaussian(12345, WL["phi_sigma"])
+        return h
+
+    def timed(h, K, W, sampler=None):
+        for _ in range(W):
+            flush.zero_()
+            h.enqueue(1)
+        torch.cuda.synchronize()
+        dist.barrier()
+        torch.cuda.synchronize()
+        if sampler:
+            sampler.start()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(K):
+            flush.zero_()
+            h.enqueue(1)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        clocks = sampler.stop() if sampler else None
+        dist.barrier()
+        ms = dist.max(e0.elapsed_time(e1))
+        return ms, clocks
+
+    def kernel_ms(h, which, n=40):
+        eps = 0.0   # zero step: the kernel does all its work but leaves the state unchanged (kick)
+        fn = h.kick if which == "kick" else h.drift
+        for _ in range(3):
+            fn(eps)
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(n):
+            fn(eps)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / n
+
+    K, W = a.steps, a.warmup
+    res = {}
+    for prec in ("fp32", "fp64"):
+        h = make(prec)
+        sampler = ClockSampler(dist.local) if prec == "fp32" else None
+        ms, clocks = timed(h, K, W, sampler)
+        recs = h.records(min(K, 1024))
+        res[prec] = dict(ms=ms, clocks=clocks, acc=float(np.mean(recs["accepted"])),
+                         plaq=float(np.mean(recs["plaquette"])), dH=float(np.mean(recs["dH"])),
+                         kick_ms=kernel_ms(h, "kick"), drift_ms=kernel_ms(h, "drift"), h=h)
+
+    V = int(np.prod(WL["L"]))
+    traj_fp32 = dist.world * K / (res["fp32"]["ms"] / 1e3)
+    traj_fp64 = dist.world * K / (res["fp64"]["ms"] / 1e3)
+
+    # ---- end to end through the public API with host-resident fields ----
+    h = res["fp32"]["h"]
+    U_host = torch.empty(V * 4 * 9 * 2, dtype=torch.float64, pin_memory=True).numpy()
+    phi_host = torch.empty(V * 3 * 2, dtype=torch.float64, pin_memory=True).numpy()
+    Uc = U_host.view(np.complex128).reshape(V, 4, 3, 3)
+    pc = phi_host.view(np.complex128).reshape(V, 3)
+    Uc[:] = h.U
+    pc[:] = h.phi
+    Ke = max(1, min(K, 50))
+    for _ in range(2):
+        h.trajectory_host(Uc, pc)
+    torch.cuda.synchronize()
+    dist.barrier()
+    t0 = time.perf_counter()
+    for _ in range(Ke):
+        h.trajectory_host(Uc, pc)
+    torch.cuda.synchronize()
+    e2e_s = dist.max(time.perf_counter() - t0)
+    e2e = {"value": dist.world * Ke / e2e_s, "unit": "trajectories/s",
+           "h2d_bytes_per_step": int(U_host.nbytes + phi_host.nbytes),
+           "d2h_bytes_per_step": int(U_host.nbytes + phi_host.nbytes + 40), "steps": Ke,
+           "api": "gh_trajectory_host (pinned host U, phi in; U, phi, record out)"}
+
+    # ---- roofline of the dominant kernel (FP32-MD path) ----
+    hbm, peak_kind = peaks()
+    r = res["fp32"]
+    share_kick = (2 * WL["nmd"] + 1) * r["kick_ms"]
+    share_drift = 2 * WL["nmd"] * r["drift_ms"]
+    dom = "kick" if share_kick >= share_drift else "drift"
+    dom_ms = r[dom + "_ms"]
+    achieved = V * ALG_BYTES[dom]["fp32"] / (dom_ms / 1e3) / 1e9
+    traffic = None
+    tp = os.path.join(ROOT, "profiles", "traffic_su3_fund_16x4.json")
+    if os.path.exists(tp):
+        with open(tp) as f:
+            traffic = json.load(f).get(f"{dom}_fp32_dram_bytes_per_launch")
+    roofline = {"bound": "hbm", "kernel": f"k_kick<4,3,float,FUND>" if dom == "kick" else "k_drift<3,float>",
+                "achieved": round(achieved, 1), "peak": hbm, "unit": "GB/s", "frac": round(achieved / hbm, 4),
+                "peak_source": peak_kind, "traffic": traffic,
+                "alg_bytes_per_launch": V * ALG_BYTES[dom]["fp32"], "avg_launch_ms": round(dom_ms, 5),
+                "share_of_trajectory": round((share_kick if dom == "kick" else share_drift) / (r["ms"] / K), 3),
+                "fp64": {"kick_ms": round(res["fp64"]["kick_ms"], 5), "drift_ms": round(res["fp64"]["drift_ms"], 5),
+                         "kick_GBps": round(V * ALG_BYTES["kick"]["fp64"] / (res["fp64"]["kick_ms"] / 1e3) / 1e9, 1)},
+                "fp32": {"kick_ms": round(r["kick_ms"], 5), "drift_ms": round(r["drift_ms"], 5)}}
+
+    # ---- CPU baseline: the reference itself on this host's cores (rank 0, N=1) ----
+    cpu = None
+    if dist.world == 1 and not a.no_cpu:
+        cpu = cpu_baseline(n_traj=a.cpu_traj)
+
+    line = {
+        "metric": METRIC, "value": round(traj_fp32, 3), "unit": "trajectories/s", "n_gpus": dist.world,
+        "steps": K, "warmup": W, "ms_per_step": round(res["fp32"]["ms"] / K, 4), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (reference counter-RNG hot start and Gaussian scalar field)",
+        "config": {"workload": WORKLOAD, "lattice": WL["L"], "rep": "fundamental", "beta": WL["beta"],
+                   "kappa": WL["kappa"], "lambda": WL["lam"], "integrator": "omelyan", "nmd": WL["nmd"],
+                   "tau": WL["tau"], "precision": "FP32 MD forces and links; FP64 H, exp(iH), reunitarisation",
+                   "l2": "flushed between trajectories (256 MB write, inside the timed region)",
+                   "parallelism": f"replicas x{dist.world}"},
+        "fp64": {"value": round(traj_fp64, 3), "ms_per_step": round(res["fp64"]["ms"] / K, 4),
+                 "acceptance": res["fp64"]["acc"], "plaquette": res["fp64"]["plaq"]},
+        "fp32_over_fp64": round(traj_fp32 / traj_fp64, 3),
+        "acceptance": res["fp32"]["acc"], "plaquette": res["fp32"]["plaq"],
+        "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
+        "gpu_launches": K * launches_per_traj(WL["nmd"], "fp32"),
+        "clocks": res["fp32"]["clocks"],
+    }
+    for p in ("fp32", "fp64"):
+        res[p]["h"].close()
+    dist.close()
+    if dist.rank == 0:
+        print(json.dumps(line))
+
+
+def cpu_baseline(n_traj=2):
+    """The reference (oracle/_ref/libghref.so: the unmodified reference headers) on all
+    host cores, timing its own GaugeHiggsHMC::trajectory() loop on the bench workload."""
+    from oracle.oracle import Reference, RefSession, have_reference, OMELYAN
+    if not have_reference():
+        return cpu_baseline_port()
+    ref = Reference()
+    cores = ref.set_threads(os.cpu_count() or 1)
+    s = RefSession(ref, WL["D"], WL["N"], WL["L"], WL["spec"], WL["beta"], WL["kappa"], WL["lam"], WL["nmd"],
+                   WL["tau"], 1, OMELYAN, WL["hot_sigma"], WL["phi_sigma"])
+    t0 = time.perf_counter()
+    s.run(n_traj)
+    dt = time.perf_counter() - t0
+    s.close()
+    return {"value": round(n_traj / dt, 5), "unit": "trajectories/s", "cores": cores, "kind": "reference",
+            "sample": f"{n_traj} trajectories of the bench workload (setup excluded), OpenMP {cores} threads, "
+                      f"{dt:.1f} s"}
+
+
+def cpu_baseline_port():
+    from oracle.oracle import Oracle, REP_FUND, OMELYAN
+    o = Oracle()
+    rep = o.rep(REP_FUND, 3)
+    h = o.hmc(4, 3, WL["L"], rep, seed=1, beta=WL["beta"], kappa=WL["kappa"], lam=WL["lam"], nmd=WL["nmd"],
+              integ=OMELYAN)
+    h.U[:] = o.hot_start(4, 3, WL["L"], 1, 0.8)
+    t0 = time.perf_counter()
+    h.trajectory()
+    dt = time.perf_counter() - t0
+    return {"value": round(1 / dt, 5), "unit": "trajectories/s", "cores": 1, "kind": "port",
+            "sample": f"1 trajectory of the bench workload on the C restatement, {dt:.1f} s"}
+
+
+def run_reference(a, dist):
+    """Reference arm: the reference's own CPU implementation, all host threads, rank 0 only."""
+    if dist.rank != 0:
+        return
+    from oracle.oracle import Reference, RefSession, have_reference, OMELYAN
+    if not have_reference():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libghref.so was not built"}))
+        return
+    ref = Reference()
+    cores = ref.set_threads(os.cpu_count() or 1)
+    s = RefSession(ref, WL["D"], WL["N"], WL["L"], WL["spec"], WL["beta"], WL["kappa"], WL["lam"], WL["nmd"],
+                   WL["tau"], 1, OMELYAN, WL["hot_sigma"], WL["phi_sigma"])
+    t0 = time.perf_counter()
+    s.run(max(1, min(a.warmup, 1)))
+    t_first = time.perf_counter() - t0
+    # bound the whole run to a few minutes: at most ~150 s of timed trajectories
+    K = max(1, min(a.steps, int(150.0 / max(t_first, 1e-3))))
+    t0 = time.perf_counter()
+    s.run(K)
+    dt = time.perf_counter() - t0
+    acc = s.acceptance()
+    s.close()
+    v = K / dt
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": round(v, 5), "unit": "trajectories/s", "n_gpus": dist.world,
+        "steps": K, "steps_requested": a.steps, "warmup": 1, "ms_per_step": round(dt / K * 1e3, 2),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (reference counter-RNG hot start and Gaussian scalar field)",
+        "config": {"workload": WORKLOAD, "lattice": WL["L"], "rep": "fundamental", "beta": WL["beta"],
+                   "kappa": WL["kappa"], "lambda": WL["lam"], "integrator": "omelyan", "nmd": WL["nmd"],
+                   "tau": WL["tau"], "precision": "FP64 (reference)", "parallelism": f"OpenMP {cores} threads"},
+        "acceptance": acc,
+        "cpu_baseline": {"value": round(v, 5), "unit": "trajectories/s", "cores": cores, "kind": "reference",
+                         "sample": f"{K} trajectories of the bench workload via GaugeHiggsHMC::trajectory()"},
+        "e2e": {"value": round(v, 5), "unit": "trajectories/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--cpu-traj", type=int, default=3)
+    ap.add_argument("--no-cpu", action="store_true")
+    a = ap.parse_args()
+    if a.warmup < 3 and a.impl == "ours":
+        a.warmup = 3
+    dist = Dist()
+    if a.impl == "reference":
+        run_reference(a, dist)
+    else:
+        run_ours(a, dist)
+
+
+if __name__ == "__main__":
+    main()

@@ -79,6 +79,8 @@ SIGNATURES = {
     "gh_trajectory": [_ctx, _dp, _ip],
     "gh_run_trajectories": [_ctx, C.c_int, C.POINTER(TrajRecord)],
     "gh_trajectory_host": [_ctx, _dp, _dp, C.POINTER(TrajRecord)],
+    "gh_enqueue_trajectories": [_ctx, C.c_int],
+    "gh_read_records": [_ctx, C.c_int, C.POINTER(TrajRecord)],
     "gh_use_graph": [_ctx, C.c_int],
     "gh_temper_enable": [_ctx, C.c_int, C.c_uint64],
     "gh_temper_stats": [_ctx, _u64p, _u64p, _dp],

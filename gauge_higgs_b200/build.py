@@ -1,6 +1,8 @@
 """Build libgauge_higgs_b200.so in-tree (gauge_higgs_b200/lib/) for sm_100a.
 
-    python -m gauge_higgs_b200.build [--force] [-j N]
+    python gauge_higgs_b200/build.py [--force] [-j N]
+
+(run by path: importing the package first would load the previous library)
 
 Each CUDA translation unit is compiled by nvcc with
 `-gencode arch=compute_100a,code=sm_100a -lineinfo -O3`; the host-only rep

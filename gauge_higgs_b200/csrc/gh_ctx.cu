@@ -731,6 +731,33 @@ int gh_run_trajectories(gh_ctx* ctx, int ntraj, gh_traj_record* records) {
   return launch_check(ctx, "run_trajectories");
 }
 
+int gh_enqueue_trajectories(gh_ctx* ctx, int ntraj) {
+  if (!ctx) return fail(nullptr, GH_ERR_ARG, "null context");
+  if (ntraj < 0) return fail(ctx, GH_ERR_ARG, "ntraj < 0");
+  for (int t = 0; t < ntraj; ++t) { int rc = run_traj(ctx); if (rc) return rc; }
+  return GH_OK;
+}
+
+int gh_read_records(gh_ctx* ctx, int ntraj, gh_traj_record* records) {
+  if (!ctx) return fail(nullptr, GH_ERR_ARG, "null context");
+  const int cap = ctx->b.hist_cap;
+  if (ntraj < 0 || ntraj > cap || !records) return fail(ctx, GH_ERR_ARG, "need 0 <= ntraj <= 1024 and an output array");
+  std::vector<TrajRec> h((size_t)ctx->nlat * cap);
+  std::vector<LatDev> L(ctx->nlat);
+  CK(cudaMemcpyAsync(L.data(), ctx->b.lats, sizeof(LatDev) * ctx->nlat, cudaMemcpyDeviceToHost, ctx->st));
+  CK(cudaMemcpyAsync(h.data(), ctx->b.hist, sizeof(TrajRec) * h.size(), cudaMemcpyDeviceToHost, ctx->st));
+  CK(cudaStreamSynchronize(ctx->st));
+  for (int l = 0; l < ctx->nlat; ++l)
+    for (int t = 0; t < ntraj; ++t) {
+      gh_traj_record& o = records[(size_t)t * ctx->nlat + l];
+      if (L[l].traj < (unsigned long long)(ntraj - t)) { std::memset(&o, 0, sizeof(o)); continue; }
+      const unsigned long long tr = L[l].traj - (unsigned long long)(ntraj - t);
+      const TrajRec& r = h[(size_t)l * cap + (int)(tr % (unsigned long long)cap)];
+      o.dH = r.dH; o.accepted = r.accepted; o.traj = r.traj; o.plaquette = r.plaq; o.L_phi = r.L_phi; o.L_link = r.L_link;
+    }
+  return GH_OK;
+}
+
 int gh_trajectory_host(gh_ctx* ctx, double* U, double* phi, gh_traj_record* rec) {
   if (!ctx) return fail(nullptr, GH_ERR_ARG, "null context");
   if (ctx->nlat != 1) return fail(ctx, GH_ERR_ARG, "gh_trajectory_host needs a single-lattice context");

@@ -321,6 +321,18 @@ class Ensemble:
         arr = np.frombuffer(recs, dtype=dt, count=ntraj * self.n_lat).copy()
         return arr.reshape(ntraj, self.n_lat)
 
+    def enqueue(self, ntraj=1):
+        """Enqueue trajectories on the context stream without synchronising."""
+        self.ctx("gh_enqueue_trajectories", int(ntraj))
+
+    def records(self, ntraj):
+        """Records of the last ntraj (<= 1024) trajectories, [ntraj, n_lat]."""
+        recs = (TrajRecord * (ntraj * self.n_lat))()
+        self.ctx("gh_read_records", int(ntraj), recs)
+        dt = np.dtype([("dH", "f8"), ("accepted", "i4"), ("traj", "i4"), ("plaquette", "f8"), ("L_phi", "f8"),
+                       ("L_link", "f8")])
+        return np.frombuffer(recs, dtype=dt, count=ntraj * self.n_lat).copy().reshape(ntraj, self.n_lat)
+
     def use_graph(self, on=True):
         self.ctx("gh_use_graph", int(bool(on)))
 

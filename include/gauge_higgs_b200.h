@@ -169,6 +169,12 @@ int gh_trajectory(gh_ctx* ctx, double* dH, int* accepted);
 /* ntraj trajectories back to back without host synchronisation in between;
  * records: ntraj * n_lat entries [t][lat] (may be NULL). */
 int gh_run_trajectories(gh_ctx* ctx, int ntraj, gh_traj_record* records);
+/* Enqueue ntraj trajectories on the context's stream and return without
+ * synchronising (records stay in the device ring of the last 1024 trajectories
+ * per lattice; read them with gh_read_records after gh_sync). */
+int gh_enqueue_trajectories(gh_ctx* ctx, int ntraj);
+/* The records of the last ntraj (<= 1024) trajectories: ntraj * n_lat entries [t][lat]. */
+int gh_read_records(gh_ctx* ctx, int ntraj, gh_traj_record* records);
 /* Host-resident fields (single lattice): upload U and phi, run one trajectory,
  * download U, phi and the record.  The drop-in for a driver that keeps the
  * fields in host memory like the reference's GaugeField / CVecField. */

@@ -379,6 +379,13 @@ class Reference:
                               _dp, _dp]
         L.ref_set_threads.argtypes = [C.c_int]
         L.ref_set_threads.restype = C.c_int
+        L.ref_session_create.restype = C.c_void_p
+        L.ref_session_create.argtypes = [C.c_int, C.c_int, _ip, C.c_char_p, C.c_double, C.c_double, C.c_double,
+                                         C.c_int, C.c_double, _u64, C.c_int, C.c_double, C.c_double]
+        L.ref_session_run.argtypes = [C.c_void_p, C.c_int, _dp]
+        L.ref_session_acceptance.restype = C.c_double
+        L.ref_session_acceptance.argtypes = [C.c_void_p]
+        L.ref_session_destroy.argtypes = [C.c_void_p]
 
     @staticmethod
     def _L(L):
@@ -536,6 +543,34 @@ class Reference:
         if rc:
             raise RuntimeError(f"ref_run rc={rc}")
         return series[:nmeas], acc.value
+
+
+class RefSession:
+    """A persistent reference GaugeHiggsHMC driven by its own trajectory() loop."""
+
+    def __init__(self, ref, D, N, L, spec, beta, kappa, lam, nmd, tau, seed, integ=OMELYAN, hot_sigma=0.8,
+                 phi_sigma=0.3):
+        self.lib = ref.lib
+        self.h = self.lib.ref_session_create(D, N, Reference._L(L), spec.encode(), beta, kappa, lam, nmd, tau, seed,
+                                             integ, hot_sigma, phi_sigma)
+        if not self.h:
+            raise RuntimeError("unsupported reference session configuration")
+
+    def run(self, ntraj, series=False):
+        out = np.zeros((max(ntraj, 1), 5)) if series else None
+        self.lib.ref_session_run(self.h, ntraj, _d(out) if series else None)
+        return out[:ntraj] if series else None
+
+    def acceptance(self):
+        return self.lib.ref_session_acceptance(self.h)
+
+    def close(self):
+        if self.h:
+            self.lib.ref_session_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
 
 
 def have_reference(path=REF_SO):

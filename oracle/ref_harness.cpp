@@ -280,3 +280,48 @@ int ref_run(int D, int N, const int* L, const char* spec, double beta, double ka
 }
 
 }  // extern "C"
+
+// ---- a persistent reference HMC object: the reference driver's own loop of
+// GaugeHiggsHMC::trajectory() (src/hmc_higgs.cpp:72-87), one call per step ----
+struct RefSession {
+  virtual ~RefSession() {}
+  virtual int run(int ntraj, double* series) = 0;   // series: [ntraj][5] as ref_run
+  virtual double acceptance() = 0;
+};
+template <int DD, int NN>
+struct RefSessionT : RefSession {
+  const Representation<NN>* r;
+  GaugeHiggsHMC<DD, NN> h;
+  RefSessionT(const int* L, const Representation<NN>* rep, uint64_t seed) : r(rep), h(ext<DD>(L), *rep, seed) {}
+  int run(int ntraj, double* series) override {
+    for (int t = 0; t < ntraj; ++t) {
+      h.trajectory();
+      if (series) {
+        double* o = series + 5 * t;
+        o[0] = avg_plaquette<DD, NN>(h.U); o[1] = higgs_length<DD>(h.phi); o[2] = link_energy<DD, NN>(h.phi, h.U, *r);
+        o[3] = polyakov_loop<DD, NN>(h.U); o[4] = h.last_dH;
+      }
+    }
+    return 0;
+  }
+  double acceptance() override { return h.acceptance(); }
+};
+
+extern "C" {
+
+void* ref_session_create(int D, int N, const int* L, const char* spec, double beta, double kappa, double lambda,
+                         int nmd, double tau, uint64_t seed, int integ, double hot_sigma, double phi_sigma) {
+  RefSession* s = nullptr;
+#define CALL(DD, NN) { auto* r = get_rep<NN>(spec); if (!r) return nullptr; auto* t = new RefSessionT<DD, NN>(L, r, seed); \
+    t->h.beta = beta; t->h.kappa = kappa; t->h.lambda = lambda; t->h.nmd = nmd; t->h.tau = tau; \
+    t->h.integ = integ == 0 ? Integrator::Leapfrog : Integrator::Omelyan2MN; \
+    t->h.U.hot(t->h.rng, hot_sigma); t->h.phi.gaussian(t->h.rng, 12345, r->real, phi_sigma); s = t; }
+  if (D == 4 && N == 3) CALL(4, 3) else if (D == 4 && N == 2) CALL(4, 2) else if (D == 3 && N == 3) CALL(3, 3) else if (D == 3 && N == 2) CALL(3, 2)
+#undef CALL
+  return s;
+}
+int ref_session_run(void* s, int ntraj, double* series) { return s ? static_cast<RefSession*>(s)->run(ntraj, series) : -1; }
+double ref_session_acceptance(void* s) { return s ? static_cast<RefSession*>(s)->acceptance() : 0.0; }
+void ref_session_destroy(void* s) { delete static_cast<RefSession*>(s); }
+
+}  // extern "C"

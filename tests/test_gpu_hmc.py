@@ -1,0 +1,268 @@
+"""Integrator-level and statistical checks on the GPU, mirroring the reference's
+own tests: test/test_gauge.cpp (force FD, reversibility, dH scaling, <exp(-dH)>),
+test/test_scalar.cpp (scalar / link force FD, combined reversibility and
+<exp(-dH)>), test/test_general.cpp (general irreps), with the same tolerances,
+run in FP64 and in the FP32-MD mode."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def cube(D, n):
+    return [n] * D
+
+
+def expi_np(H):
+    w, v = np.linalg.eigh(H)
+    return (v * np.exp(1j * w)) @ v.conj().T
+
+
+def gens(N):
+    from oracle.oracle import Oracle
+    return Oracle().generators(N)
+
+
+def make(kind, D, N, precision="fp64", seed=1, **kw):
+    import gauge_higgs_b200 as gh
+    if kind == "none":
+        kw.pop("kappa", None)
+        kw.pop("lam", None)
+        return gh.GaugeHMC(cube(D, 4), N, seed=seed, precision=precision, **kw)
+    rep = {"fund": lambda: gh.FundamentalRep(N), "adj": lambda: gh.AdjointRep(N),
+           "gen2": lambda: gh.GeneralRep(N, [2]), "gen2r": lambda: gh.GeneralRep(N, [2], real=True)}[kind]()
+    return gh.GaugeHiggsHMC(cube(D, 4), rep, seed=seed, precision=precision, **kw)
+
+
+# ---------------------------------------------------------------------------
+# finite differences (test_gauge.cpp:12-49, test_scalar.cpp:64-120)
+# ---------------------------------------------------------------------------
+@pytest.mark.parametrize("D,N,kind", [(2, 2, "none"), (3, 2, "none"), (4, 2, "none"), (3, 3, "none"),
+                                      (3, 2, "fund"), (3, 2, "adj"), (3, 3, "fund"), (3, 3, "gen2")])
+def test_link_force_finite_difference(D, N, kind):
+    h = make(kind, D, N, beta=2.0, kappa=0.35, lam=0.4)
+    h.hot(0.5)
+    if kind != "none":
+        h.phi_gaussian(77, 0.7)
+    U0 = h.U
+    F = h.gauge_force() + (h.matter_link_force() if kind != "none" else 0.0)
+    T = gens(N)
+    eps = 1e-5
+    worst = 0.0
+    V = U0.shape[0]
+    for s in (0, V // 2, V - 1):
+        for mu in range(D):
+            for a in range(N * N - 1):
+                U = U0.copy()
+                U[s, mu] = expi_np(eps * T[a]) @ U0[s, mu]
+                h.U = U
+                m = h.measure()
+                Sp = m["S_g"] + m["S_H"]
+                U[s, mu] = expi_np(-eps * T[a]) @ U0[s, mu]
+                h.U = U
+                m = h.measure()
+                Sm = m["S_g"] + m["S_H"]
+                worst = max(worst, abs((Sp - Sm) / (2 * eps) - F[s, mu, a]))
+    assert worst < 1e-5 if kind != "none" else worst < 1e-6
+    h.close()
+
+
+@pytest.mark.parametrize("N,kind", [(2, "fund"), (2, "adj"), (3, "fund"), (3, "adj"), (3, "gen2")])
+def test_scalar_force_finite_difference(N, kind):
+    h = make(kind, 3, N, kappa=0.3, lam=0.4)
+    h.hot(0.5)
+    h.phi_gaussian(99, 0.7)
+    phi0 = h.phi
+    F = h.scalar_force()
+    eps = 1e-5
+    worst = 0.0
+    real = h.rep.real
+    for s in (0, 3, phi0.shape[0] - 1):
+        for k in range(phi0.shape[1]):
+            for unit in ((1.0,) if real else (1.0, 1j)):
+                p = phi0.copy()
+                p[s, k] += eps * unit
+                h.phi = p
+                Sp = h.measure()["S_H"]
+                p[s, k] -= 2 * eps * unit
+                h.phi = p
+                Sm = h.measure()["S_H"]
+                fd = -(Sp - Sm) / (2 * eps)
+                got = F[s, k].real if unit == 1.0 else F[s, k].imag
+                worst = max(worst, abs(fd - got))
+    assert worst < 1e-5
+    h.close()
+
+
+# ---------------------------------------------------------------------------
+# reversibility (test_gauge.cpp:65-85, test_scalar.cpp:122-141)
+# ---------------------------------------------------------------------------
+@pytest.mark.parametrize("precision,tol", [("fp64", 1e-9), ("fp32", 2e-4)])
+@pytest.mark.parametrize("N,kind", [(2, "none"), (3, "none"), (2, "fund"), (2, "adj"), (3, "fund"), (3, "gen2")])
+def test_reversibility(N, kind, precision, tol):
+    h = make(kind, 3, N, precision=precision, seed=999, beta=2.3, kappa=0.3, lam=0.5, nmd=12)
+    h.hot(0.5)
+    if kind != "none":
+        h.phi_gaussian(1, 0.6)
+        h.refresh_momenta()
+    else:
+        h.mom_refresh(7)
+    U0 = h.U
+    phi0 = h.phi if kind != "none" else None
+    h.md_evolve()
+    h.P = -h.P
+    if kind != "none":
+        h.pi = -h.pi
+    h.md_evolve()
+    U1 = h.U
+    worst = np.abs(U1 - U0).max()
+    if kind != "none":
+        worst = max(worst, np.abs(h.phi - phi0).max())
+    assert worst < tol, worst
+    h.close()
+
+
+# ---------------------------------------------------------------------------
+# dH second-order scaling (test_gauge.cpp:88-107)
+# ---------------------------------------------------------------------------
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_dH_scaling(precision):
+    def run(nmd):
+        h = make("none", 3, 2, precision=precision, seed=31415, beta=2.3, nmd=nmd)
+        h.hot(0.4)
+        h.mom_refresh(5)
+        Hi = h.hamiltonian()
+        h.md_evolve()
+        d = abs(h.hamiltonian() - Hi)
+        h.close()
+        return d
+    ratio = run(8) / run(16)
+    assert 3.0 < ratio < 5.0, ratio
+
+
+# ---------------------------------------------------------------------------
+# <exp(-dH)> = 1 and acceptance (test_gauge.cpp:110-129, test_scalar.cpp:143-156,
+# test_general.cpp:183-195)
+# ---------------------------------------------------------------------------
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+@pytest.mark.parametrize("N,kind,seed", [(2, "none", 2024), (3, "none", 2025), (2, "fund", 501), (2, "adj", 502),
+                                         (3, "gen2", 42)])
+def test_exp_minus_dH(N, kind, seed, precision):
+    import gauge_higgs_b200 as gh
+    if kind == "none":
+        h = make(kind, 3, N, precision=precision, seed=seed, beta=2.3, nmd=16)
+        h.hot(0.3)
+        tol, amin = 0.12, 0.55
+    else:
+        kap = 0.15 if kind == "gen2" else 0.2
+        h = make(kind, 3, N, precision=precision, seed=seed, beta=2.3, kappa=kap, lam=0.5, nmd=20)
+        h.hot(0.3)
+        h.phi_cold(0.4 if kind == "gen2" else 0.5)
+        tol, amin = 0.15, 0.5
+    ntraj = 300 if kind == "gen2" else 400
+    rec = h.run(ntraj)[:, 0]
+    mean = float(np.mean(np.exp(-rec["dH"])))
+    acc = float(np.mean(rec["accepted"]))
+    assert abs(mean - 1.0) < tol, (mean, acc)
+    if kind != "gen2":
+        assert acc > amin, acc
+    t, a, nonfinite = h.traj_counts(0)
+    assert t == ntraj and a == int(np.sum(rec["accepted"])) and nonfinite == 0
+    h.close()
+
+
+# ---------------------------------------------------------------------------
+# FP32-MD against FP64: forces, one MD trajectory, statistics at equal couplings
+# ---------------------------------------------------------------------------
+def test_fp32_force_error():
+    import gauge_higgs_b200 as gh
+    L = [6, 6, 6, 6]
+    hs = {p: gh.GaugeHiggsHMC(L, gh.FundamentalRep(3), seed=5, precision=p, beta=5.7, kappa=0.1, lam=0.5)
+          for p in ("fp64", "fp32")}
+    hs["fp64"].hot(0.8)
+    hs["fp64"].phi_gaussian(12345, 0.3)
+    U, phi = hs["fp64"].U, hs["fp64"].phi
+    hs["fp32"].U = U
+    hs["fp32"].phi = phi
+    for f in ("gauge_force", "matter_link_force", "scalar_force"):
+        a = getattr(hs["fp64"], f)()
+        b = getattr(hs["fp32"], f)()
+        rel = np.abs(a - b).max() / np.abs(a).max()
+        assert rel < 5e-6, (f, rel)
+    for h in hs.values():
+        h.close()
+
+
+def test_fp32_fp64_trajectory_agreement():
+    """Same start, same momenta (bit-identical RNG in both modes): dH and the final
+    fields of one trajectory agree to FP32 accuracy."""
+    import gauge_higgs_b200 as gh
+    L = [8, 8, 8, 8]
+    out = {}
+    for p in ("fp64", "fp32"):
+        h = gh.GaugeHiggsHMC(L, gh.FundamentalRep(3), seed=7, precision=p, beta=5.7, kappa=0.1, lam=0.5, nmd=16)
+        h.cold()
+        h.phi_gaussian(12345, 0.3)
+        for _ in range(3):
+            h.trajectory()   # leave the cold start
+        h.set_traj_count(0, 0, 0)
+        acc = h.trajectory()
+        out[p] = (h.last_dH, acc, h.U, h.measure()["plaquette"])
+        h.close()
+    assert abs(out["fp64"][0] - out["fp32"][0]) < 0.05 + 0.02 * abs(out["fp64"][0])
+    assert abs(out["fp64"][3] - out["fp32"][3]) < 1e-4
+
+
+# ---------------------------------------------------------------------------
+# ensembles: one context of many lattices == independent single-lattice contexts
+# ---------------------------------------------------------------------------
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_ensemble_equals_independent(precision):
+    import gauge_higgs_b200 as gh
+    ext = [[4, 4, 4, 4], [6, 4, 4, 6], [5, 5, 3, 4]]
+    kappas = [0.22, 0.25, 0.28]
+    seeds = [11, 12, 13]
+    ens = gh.Ensemble(ext, gh.FundamentalRep(2), seeds=seeds, precision=precision, beta=2.3, kappa=kappas, lam=0.5,
+                      nmd=10, integ="leapfrog")
+    ens.hot(0.8)
+    ens.phi_gaussian(12345, 0.3)
+    rec = ens.run(6)
+    for i in range(3):
+        h = gh.GaugeHiggsHMC(ext[i], gh.FundamentalRep(2), seed=seeds[i], precision=precision, beta=2.3,
+                             kappa=kappas[i], lam=0.5, nmd=10, integ="leapfrog")
+        h.hot(0.8)
+        h.phi_gaussian(12345, 0.3)
+        r1 = h.run(6)[:, 0]
+        assert np.array_equal(r1["dH"], rec[:, i]["dH"])
+        assert np.array_equal(r1["accepted"], rec[:, i]["accepted"])
+        assert np.array_equal(h.U, ens.get("U", i))
+        h.close()
+    ens.close()
+
+
+def test_tempering_toggle_and_swaps():
+    import gauge_higgs_b200 as gh
+    ext = [[4, 4, 4, 4]] * 4
+    kappas = [0.24, 0.25, 0.26, 0.27]
+    mk = lambda: gh.Ensemble(ext, gh.FundamentalRep(2), seeds=[1, 2, 3, 4], beta=2.3, kappa=kappas, lam=0.5,
+                             nmd=10, precision="fp32")
+    a = mk()
+    a.hot(0.8)
+    a.phi_gaussian(12345, 0.3)
+    ra = a.run(20)
+    b = mk()
+    b.hot(0.8)
+    b.phi_gaussian(12345, 0.3)
+    b.enable_tempering(False)
+    rb = b.run(20)
+    assert np.array_equal(ra["dH"], rb["dH"])     # toggle off: bit-identical to no tempering
+    c = mk()
+    c.hot(0.8)
+    c.phi_gaussian(12345, 0.3)
+    c.enable_tempering(True, swap_seed=0x5A7AB1EC)
+    c.run(60)
+    att, acc, kap = c.tempering_stats()
+    assert att.sum() > 0 and acc.sum() > 0
+    assert sorted(np.round(kap, 12).tolist()) == sorted(kappas)   # a permutation of the ladder
+    for x in (a, b, c):
+        x.close()
