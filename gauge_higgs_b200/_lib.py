@@ -98,6 +98,12 @@ def load(path=LIB_PATH):
         f = getattr(lib, name)
         f.argtypes = args
         f.restype = C.c_int
+    lib.gh_rng_key.argtypes = [C.c_uint64] * 5
+    lib.gh_rng_key.restype = C.c_uint64
+    lib.gh_rng_uniform.argtypes = [C.c_uint64, C.c_uint64]
+    lib.gh_rng_uniform.restype = C.c_double
+    lib.gh_rng_gauss.argtypes = [C.c_uint64, C.c_uint64]
+    lib.gh_rng_gauss.restype = C.c_double
     lib.gh_last_error.argtypes = [C.c_void_p]
     lib.gh_last_error.restype = C.c_char_p
     return lib

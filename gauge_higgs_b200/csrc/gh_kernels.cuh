@@ -155,9 +155,12 @@ struct KickArgs {
   double* out;        // M_WRITE destination (SoA like P / like phi, FP64)
 };
 
-template <int D, int N, typename R, int REP>
-__device__ __forceinline__ void kick_link(const KickArgs& a, const LatDev& L, int mu, int s) {
+// The direction is a template parameter so that every index into the lattice
+// descriptor is static (no local-memory copy of the descriptor).
+template <int D, int N, typename R, int REP, int MU>
+__device__ __forceinline__ void kick_link(const KickArgs& a, const LatDev& L, int s) {
   typedef typename Cmp<R>::t C;
+  constexpr int mu = MU;
   const R* U = (const R*)a.U;
   int x[D];
   coords<D>(L, s, x);
@@ -311,12 +314,27 @@ __device__ __forceinline__ void kick_site(const KickArgs& a, const LatDev& L, in
 }
 
 template <int D, int N, typename R, int REP>
-__global__ void __launch_bounds__(KBLOCK) k_kick(const KickArgs a) {
+__device__ __forceinline__ void kick_link_dispatch(const KickArgs& a, const LatDev& L, int mu, int s) {
+  if (mu == 0) kick_link<D, N, R, REP, 0>(a, L, s);
+  else if (mu == 1) kick_link<D, N, R, REP, 1>(a, L, s);
+  else if constexpr (D > 2) {
+    if (mu == 2) kick_link<D, N, R, REP, 2>(a, L, s);
+    else if constexpr (D > 3) kick_link<D, N, R, REP, 3>(a, L, s);
+  }
+}
+
+// Occupancy: FP32 instances are held to 128 registers (4 blocks of 128 per SM),
+// FP64 instances to 168 (3 blocks).
+template <typename R> struct KickMinBlocks { static constexpr int v = 4; };
+template <> struct KickMinBlocks<double> { static constexpr int v = 3; };
+
+template <int D, int N, typename R, int REP>
+__global__ void __launch_bounds__(KBLOCK, KickMinBlocks<R>::v) k_kick(const KickArgs a) {
   const Work w = a.work[blockIdx.x];
   if ((int)threadIdx.x >= w.n) return;
-  const LatDev L = a.lats[w.lat];
+  const LatDev& L = a.lats[w.lat];
   const int s = w.s0 + threadIdx.x;
-  if (w.mu >= 0) kick_link<D, N, R, REP>(a, L, w.mu, s);
+  if (w.mu >= 0) kick_link_dispatch<D, N, R, REP>(a, L, w.mu, s);
   else if (REP != REP_NONE) kick_site<D, N, R, REP>(a, L, s);
 }
 

@@ -225,6 +225,8 @@ template <int N, typename T> GH_HD Mat<N, T> alg_to_mat_c(const cx<T>* z) {
   return M;
 }
 
+template <int N, typename T> GH_HD cx<T> det(const Mat<N, T>& U);
+
 // ---------------------------------------------------------------------------
 // exp(iH), H Hermitian traceless, in FP64 (src/group/sun.hpp:11-45).
 // General N: scaling and squaring to ||A||_F <= 1/2, then the Taylor series,
@@ -253,6 +255,47 @@ template <int N> GH_HD Mat<N, double> expi(const Mat<N, double>& H) {
   }
   for (int i = 0; i < s; ++i) res = mm(res, res);
   return res;
+}
+// SU(3): the same Taylor series sum_n (iQ)^n / n!, Q = H / 2^s, with every power
+// reduced by the Cayley-Hamilton identity Q^3 = c1 Q + c0 I (c1 = Tr Q^2 / 2,
+// c0 = det Q for traceless Q): Q^n = a_n I + b_n Q + g_n Q^2 with
+// (a, b, g)_{n+1} = (c0 g_n, a_n + c1 g_n, b_n).  The series runs on three
+// scalars instead of 3x3 matrices; exp(iQ) = f0 I + f1 Q + f2 Q^2.
+template <> GH_HD Mat<3, double> expi<3>(const Mat<3, double>& H) {
+  double nrm = sqrt(fnorm2(H));
+  int s = 0;
+  while (nrm > 0.5) { nrm *= 0.5; ++s; }
+  const double sc = ldexp(1.0, -s);
+  Mat<3, double> Q;
+#pragma unroll
+  for (int i = 0; i < 9; ++i) Q.e[i] = scale(H.e[i], sc);
+  const Mat<3, double> Q2 = mm(Q, Q);
+  const double c1 = 0.5 * (Q2.e[0].re + Q2.e[4].re + Q2.e[8].re);
+  const double c0 = det<3, double>(Q).re;
+  double a = 1.0, b = 0.0, g = 0.0, coef = 1.0;
+  double f0r = 1.0, f0i = 0.0, f1r = 0.0, f1i = 0.0, f2r = 0.0, f2i = 0.0;
+  for (int n = 1; n <= 40; ++n) {
+    const double an = c0 * g, bn = a + c1 * g, gn = b;
+    a = an; b = bn; g = gn;
+    coef /= n;
+    const double ta = coef * a, tb = coef * b, tg = coef * g;
+    switch (n & 3) {   // i^n = 1, i, -1, -i
+      case 0: f0r += ta; f1r += tb; f2r += tg; break;
+      case 1: f0i += ta; f1i += tb; f2i += tg; break;
+      case 2: f0r -= ta; f1r -= tb; f2r -= tg; break;
+      default: f0i -= ta; f1i -= tb; f2i -= tg; break;
+    }
+    if (fabs(ta) + fabs(tb) + fabs(tg) < 1e-18) break;
+  }
+  Mat<3, double> E;
+#pragma unroll
+  for (int i = 0; i < 9; ++i)
+    E.e[i] = add(mul(mk<double>(f1r, f1i), Q.e[i]), mul(mk<double>(f2r, f2i), Q2.e[i]));
+  E.e[0].re += f0r; E.e[0].im += f0i;
+  E.e[4].re += f0r; E.e[4].im += f0i;
+  E.e[8].re += f0r; E.e[8].im += f0i;
+  for (int i = 0; i < s; ++i) E = mm(E, E);
+  return E;
 }
 template <> GH_HD Mat<2, double> expi<2>(const Mat<2, double>& H) {
   // r^2 = Tr(H^2)/2

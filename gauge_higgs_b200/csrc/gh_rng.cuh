@@ -12,10 +12,13 @@
 // published techniques, not from any vendor library:
 //   * error-free transformations two_sum (Knuth, TAOCP vol. 2, 4.2.2) and
 //     two_prod via fused multiply-add (Dekker 1971 / Ogita-Rump-Oishi 2005);
-//   * log: x = 2^e m, m in [1/sqrt2, sqrt2), log m = 2 atanh(s), s=(m-1)/(m+1),
-//     atanh series summed by Horner in double-double (about 2^-100 relative);
-//   * cos: Cody-Waite style reduction by pi/2 held as a triple-double, then the
-//     sin/cos Taylor series in double-double on |r| <= pi/4.
+//   * table-driven argument reduction in the manner of Tang (ACM TOMS 1989/1990)
+//     with double-double tables from gen_rng_tables.py (mpmath, 400 bits);
+//   * log: x = 2^e m, m in [1/sqrt2, sqrt2), m = c (1 + r) with c = i/128,
+//     log m = log c + 2 atanh(s), s = (m - c)/(m + c), series in double-double;
+//   * cos: Cody-Waite style reduction by pi/32 held as a triple-double, then
+//     the addition formula with tabulated cos / sin(j pi/32) and the sin/cos
+//     Taylor series in double-double on |r| <= pi/64.
 // Final rounding hi+lo gives the correctly rounded result except when the true
 // value lies within ~2^-100 relative of a rounding midpoint (probability ~2^-47
 // per call).  Host and device use the same explicitly rounded operations
@@ -24,6 +27,7 @@
 #include <stdint.h>
 #include <string.h>
 #include <math.h>
+#include "gh_rng_tables.cuh"
 
 #if defined(__CUDACC__)
 #define GH_HD __host__ __device__ __forceinline__
@@ -132,50 +136,66 @@ GH_HD dd dd_div(dd x, dd y) {
   return fast_two_sum(q1, div_rn(r, y.hi));
 }
 
+// Table storage: global memory on the device (threads of a warp index it at
+// random, which constant memory would serialise), static arrays on the host.
+#if defined(__CUDACC__)
+static __device__ const double g_logc_d[] = {GH_TAB_LOGC};
+static __device__ const double g_cos_d[] = {GH_TAB_COS};
+static __device__ const double g_sin_d[] = {GH_TAB_SIN};
+static __device__ const double g_odd_d[] = {GH_TAB_ODD};
+static __device__ const double g_cfac_d[] = {GH_TAB_CFAC};
+static __device__ const double g_sfac_d[] = {GH_TAB_SFAC};
+#endif
+static const double g_logc_h[] = {GH_TAB_LOGC};
+static const double g_cos_h[] = {GH_TAB_COS};
+static const double g_sin_h[] = {GH_TAB_SIN};
+static const double g_odd_h[] = {GH_TAB_ODD};
+static const double g_cfac_h[] = {GH_TAB_CFAC};
+static const double g_sfac_h[] = {GH_TAB_SFAC};
+#if defined(__CUDA_ARCH__)
+#define GH_TAB(name, i) dd{__ldg(&g_##name##_d[2 * (i)]), __ldg(&g_##name##_d[2 * (i) + 1])}
+#else
+#define GH_TAB(name, i) dd{g_##name##_h[2 * (i)], g_##name##_h[2 * (i) + 1]}
+#endif
+
 // log x for finite normal x > 0, correctly rounded (see header).
+// x = 2^e m, m in [1/sqrt2, sqrt2); c = i/128 nearest to m (i = 91..181);
+// log m = log c + 2 atanh(s), s = (m - c)/(m + c), |s| < 0.0028 (7 series terms).
 GH_HD double cr_log(double x) {
-  uint64_t bits = dbits(x);
+  const uint64_t bits = dbits(x);
   int e = (int)((bits >> 52) & 0x7FF) - 1023;
   double m = bitsd((bits & 0x000FFFFFFFFFFFFFULL) | 0x3FF0000000000000ULL);  // m in [1,2)
-  if (m > 1.4142135623730951) { m = mul_rn(m, 0.5); e += 1; }      // m in [1/sqrt2, sqrt2)
-  const double num = sub_rn(m, 1.0);                                  // exact (Sterbenz)
-  const dd den = two_sum(m, 1.0);
-  const dd s = dd_div(dd{num, 0.0}, den);
+  if (m > 1.4142135623730951) { m = mul_rn(m, 0.5); e += 1; }                 // exact
+  const double ci = rint_rn(mul_rn(m, 128.0));
+  const int i = (int)ci;
+  const double c = mul_rn(ci, 0.0078125);                                      // i/128, exact
+  const double t = sub_rn(m, c);                                               // exact, |t| <= 1/256
+  const dd s = dd_div(dd{t, 0.0}, two_sum(mul_rn(2.0, c), t));
   const dd z = dd_mul(s, s);
-  const int K = 23;                                                   // |s| <= 0.1716: z^K/(2K+1) < 2^-120
-  dd acc = dd_div_d(dd{1.0, 0.0}, (double)(2 * K + 1));
-  for (int j = K - 1; j >= 0; --j)
-    acc = dd_add(dd_div_d(dd{1.0, 0.0}, (double)(2 * j + 1)), dd_mul(z, acc));
-  const dd logm = dd_mul(dd_mul_d(s, 2.0), acc);
-  const dd ln2{0.6931471805599453, 2.3190468138462996e-17};           // ln 2 = hi + lo (to ~2^-107)
-  const dd r = dd_add(dd_mul_d(ln2, (double)e), logm);
+  dd acc = GH_TAB(odd, 7);
+  for (int j = 6; j >= 0; --j) acc = dd_add(GH_TAB(odd, j), dd_mul(z, acc));
+  const dd lm = dd_add(GH_TAB(logc, i - 90), dd_mul(dd_mul_d(s, 2.0), acc));
+  const dd r = dd_add(dd_mul_d(dd{GH_LN2_HI, GH_LN2_LO}, (double)e), lm);
   return add_rn(r.hi, r.lo);
 }
 
 // cos x for |x| < 2^20, correctly rounded (see header).
+// x = k pi/32 + r, |r| <= pi/64 (pi/32 as a triple-double); with j = k mod 64,
+// cos x = cos(j pi/32) cos r - sin(j pi/32) sin r, series to z^9 (z = r^2).
 GH_HD double cr_cos(double x) {
-  const double P1 = 1.5707963267948966, P2 = 6.123233995736766e-17, P3 = -1.4973849048591698e-33;
-  const double k = rint_rn(mul_rn(x, 0.6366197723675814));
-  dd r = dd_add(dd{x, 0.0}, dd_neg(two_prod(k, P1)));
-  r = dd_add(r, dd_neg(two_prod(k, P2)));
-  r = dd_add(r, dd{-mul_rn(k, P3), 0.0});
-  const int q = ((int)k) & 3;
+  const double k = rint_rn(mul_rn(x, GH_32_OVER_PI));
+  dd r = dd_add(dd{x, 0.0}, dd_neg(two_prod(k, GH_PI32_1)));
+  r = dd_add(r, dd_neg(two_prod(k, GH_PI32_2)));
+  r = dd_add(r, dd{-mul_rn(k, GH_PI32_3), 0.0});
+  const int j = ((int)k) & 63;
   const dd z = dd_mul(r, r);
-  const int J = 16;                      // |r| <= pi/4: z^J/(2J)! < 2^-125
-  dd cc[J + 1], ss[J + 1];
-  cc[0] = dd{1.0, 0.0};
-  ss[0] = dd{1.0, 0.0};
-  for (int j = 1; j <= J; ++j) {
-    cc[j] = dd_div_d(cc[j - 1], -(double)((2 * j - 1) * (2 * j)));
-    ss[j] = dd_div_d(ss[j - 1], -(double)((2 * j) * (2 * j + 1)));
+  dd ca = GH_TAB(cfac, 9), sa = GH_TAB(sfac, 9);
+  for (int q = 8; q >= 0; --q) {
+    ca = dd_add(GH_TAB(cfac, q), dd_mul(z, ca));
+    sa = dd_add(GH_TAB(sfac, q), dd_mul(z, sa));
   }
-  dd cacc = cc[J], sacc = ss[J];
-  for (int j = J - 1; j >= 0; --j) {
-    cacc = dd_add(cc[j], dd_mul(z, cacc));
-    sacc = dd_add(ss[j], dd_mul(z, sacc));
-  }
-  sacc = dd_mul(r, sacc);
-  dd res = (q == 0) ? cacc : (q == 1) ? dd_neg(sacc) : (q == 2) ? dd_neg(cacc) : sacc;
+  sa = dd_mul(r, sa);
+  const dd res = dd_add(dd_mul(GH_TAB(cos, j), ca), dd_neg(dd_mul(GH_TAB(sin, j), sa)));
   return add_rn(res.hi, res.lo);
 }
 

@@ -195,6 +195,14 @@ int gh_temper_enable(gh_ctx* ctx, int mode, uint64_t swap_seed);
  * kappa_of_lat: current kappa of each lattice. */
 int gh_temper_stats(gh_ctx* ctx, uint64_t* attempts, uint64_t* accepts, double* kappa_of_lat);
 
+/* ---- the counter RNG on the host (src/core/rng.hpp:11-46) ----
+ * Same bits as the device kernels: key and uniform are integer exact; gauss is the
+ * correctly rounded evaluation of sqrt(-2 log u1) cos(2 pi u2).  Pure functions
+ * (they return the value, not a status). */
+uint64_t gh_rng_key(uint64_t a, uint64_t b, uint64_t c, uint64_t d, uint64_t e);
+double gh_rng_uniform(uint64_t seed, uint64_t key);
+double gh_rng_gauss(uint64_t seed, uint64_t key);
+
 /* ---- general irreps: host-side construction of the GeneralRep tables ----
  * The Young-symmetriser basis of src/rep/rep_general.hpp:54-84,338-411, so a
  * driver without the reference headers can still form gh_rep_desc.
