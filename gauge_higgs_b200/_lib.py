@@ -86,6 +86,7 @@ SIGNATURES = {
     "gh_temper_stats": [_ctx, _u64p, _u64p, _dp],
     "gh_rep_general_info": [C.c_int, _ip, C.c_int, _ip, _ip, C.POINTER(C.c_long)],
     "gh_rep_general_build": [C.c_int, _ip, C.c_int, _dp, _dp],
+    "gh_plaquette_noalloc": [C.c_int, C.c_int, _ip, C.c_void_p, C.c_void_p, C.c_void_p],
 }
 
 
@@ -104,6 +105,8 @@ def load(path=LIB_PATH):
     lib.gh_rng_uniform.restype = C.c_double
     lib.gh_rng_gauss.argtypes = [C.c_uint64, C.c_uint64]
     lib.gh_rng_gauss.restype = C.c_double
+    lib.gh_noalloc_last_error.argtypes = []
+    lib.gh_noalloc_last_error.restype = C.c_char_p
     lib.gh_last_error.argtypes = [C.c_void_p]
     lib.gh_last_error.restype = C.c_char_p
     return lib

@@ -195,6 +195,25 @@ int gh_temper_enable(gh_ctx* ctx, int mode, uint64_t swap_seed);
  * kappa_of_lat: current kappa of each lattice. */
 int gh_temper_stats(gh_ctx* ctx, uint64_t* attempts, uint64_t* accepts, double* kappa_of_lat);
 
+/* ---- allocation-free plaquette reduction ----
+ * No counterpart in the reference.  For callers that cannot allocate device
+ * memory where they measure: a driver recording its own work into a CUDA graph
+ * (cudaMalloc is not allowed during stream capture and cudaFree synchronises the
+ * device) or a program whose device memory belongs to another framework's arena.
+ * U_dev: links in device memory, the reference's AoS layout [site][mu][i][j]
+ * complex FP64; out_dev (device): out[0] = sum of Re Tr U_pl, out[1] = average
+ * plaquette (as gh_measure's plaquette).  Launches on `stream` (may be NULL) and
+ * returns without synchronising.  Allocates nothing: per-block partial sums live
+ * in a file-scope __device__ array sized for GH_NOALLOC_MAX_SITES sites (64 KiB,
+ * held by every device that loads the library until exit); larger lattices are
+ * rejected with GH_ERR_ARG.  All calls on a device share that array: calls that
+ * overlap on the GPU race.  The first call on a device looks up the array's
+ * device address with that device current: make it before any stream capture.
+ * Errors: message in gh_noalloc_last_error(). */
+#define GH_NOALLOC_MAX_SITES (8192 * 128)
+int gh_plaquette_noalloc(int D, int N, const int* L, const double* U_dev, double* out_dev, void* stream);
+const char* gh_noalloc_last_error(void);
+
 /* ---- the counter RNG on the host (src/core/rng.hpp:11-46) ----
  * Same bits as the device kernels: key and uniform are integer exact; gauss is the
  * correctly rounded evaluation of sqrt(-2 log u1) cos(2 pi u2).  Pure functions
