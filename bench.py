@@ -155,6 +155,7 @@ def run_ours(a, dist):
         h.set_stream(stream.cuda_stream)
         h.hot(WL["hot_sigma"])
         h.phi_gaussian(12345, WL["phi_sigma"])
+        h.autotune(reps=3)          # kick tile shape chosen by timing (results do not depend on it)
         return h
 
     def timed(h, K, W, sampler=None):
@@ -201,7 +202,7 @@ def run_ours(a, dist):
         sampler = ClockSampler(dist.local) if prec == "fp32" else None
         ms, clocks = timed(h, K, W, sampler)
         recs = h.records(min(K, 1024))
-        res[prec] = dict(ms=ms, clocks=clocks, acc=float(np.mean(recs["accepted"])),
+        res[prec] = dict(ms=ms, clocks=clocks, acc=float(np.mean(recs["accepted"])), tile=h.get_tile(),
                          plaq=float(np.mean(recs["plaquette"])), dH=float(np.mean(recs["dH"])),
                          kick_ms=kernel_ms(h, "kick"), drift_ms=kernel_ms(h, "drift"), h=h)
 
@@ -268,6 +269,7 @@ def run_ours(a, dist):
                    "kappa": WL["kappa"], "lambda": WL["lam"], "integrator": "omelyan", "nmd": WL["nmd"],
                    "tau": WL["tau"], "precision": "FP32 MD forces and links; FP64 H, exp(iH), reunitarisation",
                    "l2": "flushed between trajectories (256 MB write, inside the timed region)",
+                   "kick_tile": {"fp32": res["fp32"]["tile"], "fp64": res["fp64"]["tile"]},
                    "parallelism": f"replicas x{dist.world}"},
         "fp64": {"value": round(traj_fp64, 3), "ms_per_step": round(res["fp64"]["ms"] / K, 4),
                  "acceptance": res["fp64"]["acc"], "plaquette": res["fp64"]["plaq"]},

@@ -82,6 +82,9 @@ SIGNATURES = {
     "gh_enqueue_trajectories": [_ctx, C.c_int],
     "gh_read_records": [_ctx, C.c_int, C.POINTER(TrajRecord)],
     "gh_use_graph": [_ctx, C.c_int],
+    "gh_autotune": [_ctx, C.c_int, _dp],
+    "gh_set_tile": [_ctx, C.c_int, _ip],
+    "gh_get_tile": [_ctx, C.c_int, _ip],
     "gh_temper_enable": [_ctx, C.c_int, C.c_uint64],
     "gh_temper_stats": [_ctx, _u64p, _u64p, _dp],
     "gh_rep_general_info": [C.c_int, _ip, C.c_int, _ip, _ip, C.POINTER(C.c_long)],

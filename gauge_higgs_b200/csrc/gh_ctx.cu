@@ -47,8 +47,12 @@ struct gh_ctx {
   int t_ngroups = 0;
   unsigned long long* t_stats = nullptr;   // [2*nlat + 1] attempts, accepts, counter
   int* t_pairmap = nullptr;
+  // tiled kick work table (rebuilt when tile shapes change)
+  Work* wk_dev = nullptr;
+  size_t wk_cap = 0;
   ~gh_ctx() {
     if (st) cudaStreamSynchronize(st);
+    if (wk_dev) cudaFree(wk_dev);
     if (gexec) cudaGraphExecDestroy(gexec);
     if (graph) cudaGraphDestroy(graph);
     for (void* p : allocs) cudaFree(p);
@@ -254,6 +258,79 @@ int xfer_field(gh_ctx* ctx, int lat, int kind, void* dev, const double* host, bo
   return GH_OK;
 }
 
+int ceil_log2(int x) { int k = 0; while ((1 << k) < x) ++k; return k; }
+
+// Default kick tile: fill the 7 bits of a 128-thread block direction by direction
+// (direction 0 first), never wider than the lattice -- the shape of 128 consecutive sites.
+void default_tile(const int* L, int D, int* lt) {
+  int left = 7;
+  for (int mu = 0; mu < 4; ++mu) lt[mu] = 0;
+  for (int mu = 0; mu < D && left > 0; ++mu) { lt[mu] = std::min(left, ceil_log2(L[mu])); left -= lt[mu]; }
+}
+
+// Kick items of the lattices in `lats` (all when empty): for every tile, its D link
+// items (directions of one tile next to each other), then one site item per tile.
+void kick_items(const gh_ctx* ctx, const std::vector<int>& lats, std::vector<Work>& out, int& nlinks, int& nsites) {
+  std::vector<Work> links, sites;
+  const int D = ctx->D;
+  for (int l : lats) {
+    const LatDev& Ld = ctx->lat_h[l];
+    int t[4], nt[4];
+    long long ntiles = 1;
+    for (int mu = 0; mu < 4; ++mu) { t[mu] = 1 << Ld.lt[mu]; nt[mu] = mu < D ? (Ld.L[mu] + t[mu] - 1) / t[mu] : 1; ntiles *= nt[mu]; }
+    for (long long q = 0; q < ntiles; ++q) {
+      long long r = q;
+      int s0 = 0, packed = 0;
+      for (int mu = 0; mu < D; ++mu) {
+        const int o = (int)(r % nt[mu]) * t[mu];
+        r /= nt[mu];
+        s0 += o * Ld.stride[mu];
+        packed |= o << (8 * mu);
+      }
+      for (int mu = 0; mu < D; ++mu) links.push_back(Work{l, mu, s0, packed});
+      sites.push_back(Work{l, -1, s0, packed});
+    }
+  }
+  nlinks = (int)links.size();
+  nsites = (int)sites.size();
+  out = links;
+  out.insert(out.end(), sites.begin(), sites.end());
+}
+
+int upload_kick_items(gh_ctx* ctx, const std::vector<Work>& items, int nlinks, int nsites) {
+  if (items.size() > ctx->wk_cap) {
+    if (ctx->wk_dev) cudaFree(ctx->wk_dev);
+    ctx->wk_dev = nullptr;
+    ctx->wk_cap = 0;
+    CK(cudaMalloc(&ctx->wk_dev, sizeof(Work) * items.size()));
+    ctx->wk_cap = items.size();
+  }
+  CK(cudaMemcpy(ctx->wk_dev, items.data(), sizeof(Work) * items.size(), cudaMemcpyHostToDevice));
+  ctx->b.w_kick = ctx->wk_dev;
+  ctx->b.nwk_links = nlinks;
+  ctx->b.nwk_sites = nsites;
+  return GH_OK;
+}
+
+int push_tiles(gh_ctx* ctx) {
+  for (int l = 0; l < ctx->nlat; ++l)
+    CK(cudaMemcpy((char*)(ctx->b.lats + l) + offsetof(LatDev, lt), ctx->lat_h[l].lt, sizeof(int) * 4, cudaMemcpyHostToDevice));
+  return GH_OK;
+}
+
+int rebuild_kick_table(gh_ctx* ctx) {
+  CK(cudaStreamSynchronize(ctx->st));
+  int rc = push_tiles(ctx);
+  if (rc) return rc;
+  std::vector<int> all(ctx->nlat);
+  for (int l = 0; l < ctx->nlat; ++l) all[l] = l;
+  std::vector<Work> items;
+  int nl, ns;
+  kick_items(ctx, all, items, nl, ns);
+  invalidate_graph(ctx);
+  return upload_kick_items(ctx, items, nl, ns);
+}
+
 int build_general(gh_ctx* ctx, const gh_rep_desc* r) {
   const int d = r->d, N = ctx->N, ng = ctx->ng;
   const long dimT = r->dimT;
@@ -372,6 +449,9 @@ int gh_ctx_create(int D, int N, int n_lat, const int* L, const gh_rep_desc* rep,
     Ld.V = (int)V; Ld.cidx = l;
     Ld.u_off = u; Ld.p_off = p; Ld.f_off = f; Ld.g_off = g;
     Ld.beta = 2.3; Ld.kappa = 0.1; Ld.lambda = 0.5; Ld.seed = seeds[l];
+    for (int mu = 0; mu < D; ++mu)
+      if (L[l * D + mu] > 256) return fail(nullptr, GH_ERR_UNSUPPORTED, "lattice extents above 256 are not supported");
+    default_tile(L + l * D, D, Ld.lt);
     u += V * D * N * N; p += V * D * ctx->ng; f += V * ctx->d; g += (ctx->rep == REP_GEN) ? V * D * ctx->d : 0;
     ctx->lat_h.push_back(Ld);
     for (int mu = 0; mu < D; ++mu)
@@ -427,6 +507,7 @@ int gh_ctx_create(int D, int N, int n_lat, const int* L, const gh_rep_desc* rep,
   CK(cudaMemcpy(b.w_all, wall.data(), sizeof(Work) * wall.size(), cudaMemcpyHostToDevice));
   if (!wg.empty()) CK(cudaMemcpy(b.w_gen, wg.data(), sizeof(Work) * wg.size(), cudaMemcpyHostToDevice));
   CK(cudaMemcpy(b.blk_first, blk_first.data(), sizeof(int) * blk_first.size(), cudaMemcpyHostToDevice));
+  if ((rc = rebuild_kick_table(ctx))) { g_err = ctx->err; return rc; }
   if (ctx->rep == REP_GEN) {
     const size_t sm = ctx->eng->gen_smem(b);
     if (sm > 227 * 1024) { g_err = "general irrep too large for the shared-memory tensor buffer"; return GH_ERR_REP; }
@@ -685,6 +766,86 @@ int gh_polyakov(gh_ctx* ctx, int lat, int tdir, double* out) {
     first += nb;
   }
   return GH_OK;
+}
+
+int gh_set_tile(gh_ctx* ctx, int lat, const int* tile) {
+  int rc = check_lat(ctx, lat, true);
+  if (rc) return rc;
+  if (!tile) return fail(ctx, GH_ERR_ARG, "null tile");
+  int lt[4] = {0, 0, 0, 0}, sum = 0;
+  for (int mu = 0; mu < ctx->D; ++mu) {
+    if (tile[mu] < 1 || (tile[mu] & (tile[mu] - 1))) return fail(ctx, GH_ERR_ARG, "tile extents must be powers of two");
+    lt[mu] = ceil_log2(tile[mu]);
+    sum += lt[mu];
+  }
+  if (sum > 7) return fail(ctx, GH_ERR_ARG, "a tile holds at most 128 sites");
+  const int l0 = lat < 0 ? 0 : lat, l1 = lat < 0 ? ctx->nlat : lat + 1;
+  for (int l = l0; l < l1; ++l) std::memcpy(ctx->lat_h[l].lt, lt, sizeof(lt));
+  return rebuild_kick_table(ctx);
+}
+
+int gh_get_tile(gh_ctx* ctx, int lat, int* tile) {
+  int rc = check_lat(ctx, lat, false);
+  if (rc) return rc;
+  if (!tile) return fail(ctx, GH_ERR_ARG, "null tile");
+  for (int mu = 0; mu < 4; ++mu) tile[mu] = mu < ctx->D ? 1 << ctx->lat_h[lat].lt[mu] : 1;
+  return GH_OK;
+}
+
+// Choose the kick tile of every group of equal-extent lattices by timing: each
+// admissible shape (power-of-two extents, 128 sites, no wider than the lattice)
+// runs `reps` zero-step kicks on that group alone; the fastest is kept.
+int gh_autotune(gh_ctx* ctx, int reps, double* best_ms) {
+  if (!ctx) return fail(nullptr, GH_ERR_ARG, "null context");
+  if (reps < 1) reps = 3;
+  CK(cudaStreamSynchronize(ctx->st));
+  std::map<std::vector<int>, std::vector<int>> groups;
+  for (int l = 0; l < ctx->nlat; ++l) groups[std::vector<int>(ctx->lat_h[l].L, ctx->lat_h[l].L + ctx->D)].push_back(l);
+  cudaEvent_t e0, e1;
+  CK(cudaEventCreate(&e0));
+  CK(cudaEventCreate(&e1));
+  double total_best = 0.0;
+  int gi = 0;
+  for (auto& kv : groups) {
+    const std::vector<int>& ext = kv.first;
+    const std::vector<int>& lats = kv.second;
+    int maxb[4] = {0, 0, 0, 0}, summax = 0;
+    for (int mu = 0; mu < ctx->D; ++mu) { maxb[mu] = std::min(7, ceil_log2(ext[mu])); summax += maxb[mu]; }
+    const int target = std::min(7, summax);
+    double best = 1e30;
+    int best_lt[4] = {0, 0, 0, 0};
+    int lt[4] = {0, 0, 0, 0};
+    // enumerate lt in [0, maxb] per direction with sum == target
+    for (lt[0] = 0; lt[0] <= maxb[0]; ++lt[0])
+      for (lt[1] = 0; lt[1] <= maxb[1]; ++lt[1])
+        for (lt[2] = 0; lt[2] <= maxb[2]; ++lt[2])
+          for (lt[3] = 0; lt[3] <= maxb[3]; ++lt[3]) {
+            if (lt[0] + lt[1] + lt[2] + lt[3] != target) continue;
+            for (int l : lats) std::memcpy(ctx->lat_h[l].lt, lt, sizeof(lt));
+            int rc = push_tiles(ctx);
+            if (rc) return rc;
+            std::vector<Work> items;
+            int nl, ns;
+            kick_items(ctx, lats, items, nl, ns);
+            if ((rc = upload_kick_items(ctx, items, nl, ns))) return rc;
+            ctx->eng->kick(ctx->b, 0.0, M_UPDATE, F_GAUGE | F_MATTER, nullptr, true, true);
+            CK(cudaEventRecord(e0, ctx->st));
+            for (int r = 0; r < reps; ++r) ctx->eng->kick(ctx->b, 0.0, M_UPDATE, F_GAUGE | F_MATTER, nullptr, true, true);
+            CK(cudaEventRecord(e1, ctx->st));
+            CK(cudaEventSynchronize(e1));
+            if ((rc = launch_check(ctx, "autotune"))) return rc;
+            float ms = 0.f;
+            CK(cudaEventElapsedTime(&ms, e0, e1));
+            if (ms / reps < best) { best = ms / reps; std::memcpy(best_lt, lt, sizeof(lt)); }
+          }
+    for (int l : lats) std::memcpy(ctx->lat_h[l].lt, best_lt, sizeof(best_lt));
+    total_best += best;
+    ++gi;
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (best_ms) *best_ms = total_best;
+  return rebuild_kick_table(ctx);
 }
 
 int gh_use_graph(gh_ctx* ctx, int enable) {

@@ -14,6 +14,8 @@ struct Bufs {
   Work* w_gen;     // general irrep: items of GEN_WARPS links
   int nw_gen;
   int* blk_first;  // [nlat+1] first site item of each lattice (relative to the site items)
+  Work* w_kick;    // kick items over 4-D tiles (LatDev::lt): link items then site items
+  int nwk_links, nwk_sites;
   double* partials;
   double* res;
   TrajRec* hist;
@@ -55,10 +57,10 @@ struct Engine : EngineBase {
     a.lats = b.lats; a.U = b.U; a.P = b.P; a.phi = b.phi; a.pi = b.pi; a.psif = b.psif; a.psib = b.psib;
     a.eps = eps; a.mode = mode; a.flags = flags; a.d = b.d; a.out = out;
     const bool do_sites = sites && b.scalar;
-    const int first = links ? 0 : b.nw_links;
-    const int count = (links ? b.nw_links : 0) + (do_sites ? b.nw_sites : 0);
+    const int first = links ? 0 : b.nwk_links;
+    const int count = (links ? b.nwk_links : 0) + (do_sites ? b.nwk_sites : 0);
     if (count == 0) return;
-    a.work = b.w_all + first;
+    a.work = b.w_kick + first;
     k_kick<D, N, R, REP><<<count, KBLOCK, 0, b.st>>>(a);
   }
   void gen_links(const Bufs& b, double eps, int mode, double* out) override {

@@ -36,9 +36,12 @@ struct LatDev {
   unsigned long long seed;
   unsigned long long traj, accepted, nonfinite;
   int last_acc;
-  int pad;
+  int lt[4];                     // kick tile shape: log2 of the tile extent per direction
 };
-struct Work { int lat, mu, s0, n; };   // mu = -1: site item
+// Block work item.  Linear items: sites s0 .. s0+n-1.  Kick items (tiles): s0 is
+// the tile's origin site and n packs the origin coordinates, 8 bits each.
+// mu = -1 marks a site item, mu >= 0 a link item of direction mu.
+struct Work { int lat, mu, s0, n; };
 
 struct GenTables {                 // general irrep (src/rep/rep_general.hpp), sparse
   int d, n, dimT, ng;
@@ -102,6 +105,24 @@ __device__ __forceinline__ int nfwd(const LatDev& L, int s, int xm, int mu) {
 __device__ __forceinline__ int nbwd(const LatDev& L, int s, int xm, int mu) {
   return (xm > 0) ? s - L.stride[mu] : s + (L.L[mu] - 1) * L.stride[mu];
 }
+// Site of thread `tid` inside a kick tile: the tile's origin comes from the work
+// item, the offset from tid split by the power-of-two tile extents.  Threads that
+// fall outside the lattice (partial tiles) return false.
+template <int D>
+__device__ __forceinline__ bool tile_site(const LatDev& L, const Work& w, int tid, int& s, int* x) {
+  s = w.s0;
+  bool in = true;
+  int r = tid;
+#pragma unroll
+  for (int mu = 0; mu < D; ++mu) {
+    const int l = r & ((1 << L.lt[mu]) - 1);
+    r >>= L.lt[mu];
+    x[mu] = ((w.n >> (8 * mu)) & 0xFF) + l;
+    in = in && (x[mu] < L.L[mu]);
+    s += l * L.stride[mu];
+  }
+  return in && (r == 0);
+}
 
 // ---------------------------------------------------------------------------
 // Representation apply for the register-resident reps.
@@ -158,12 +179,10 @@ struct KickArgs {
 // The direction is a template parameter so that every index into the lattice
 // descriptor is static (no local-memory copy of the descriptor).
 template <int D, int N, typename R, int REP, int MU>
-__device__ __forceinline__ void kick_link(const KickArgs& a, const LatDev& L, int s) {
+__device__ __forceinline__ void kick_link(const KickArgs& a, const LatDev& L, int s, const int* x) {
   typedef typename Cmp<R>::t C;
   constexpr int mu = MU;
   const R* U = (const R*)a.U;
-  int x[D];
-  coords<D>(L, s, x);
   const int spm = nfwd(L, s, x[mu], mu);
   const Mat<N, C> Umu = ld_link<N, C>(U, L, mu, s);
   Mat<N, C> Om;
@@ -239,12 +258,10 @@ __device__ __forceinline__ void kick_link(const KickArgs& a, const LatDev& L, in
 }
 
 template <int D, int N, typename R, int REP>
-__device__ __forceinline__ void kick_site(const KickArgs& a, const LatDev& L, int s) {
+__device__ __forceinline__ void kick_site(const KickArgs& a, const LatDev& L, int s, const int* x) {
   typedef typename Cmp<R>::t C;
   const R* U = (const R*)a.U;
   const R* phi = (const R*)a.phi;
-  int x[D];
-  coords<D>(L, s, x);
   const C kap2 = C(2) * (C)L.kappa;
   if (REP == REP_FUND || REP == REP_ADJ) {
     constexpr int d = RepDim<N, REP>::d;
@@ -314,28 +331,28 @@ __device__ __forceinline__ void kick_site(const KickArgs& a, const LatDev& L, in
 }
 
 template <int D, int N, typename R, int REP>
-__device__ __forceinline__ void kick_link_dispatch(const KickArgs& a, const LatDev& L, int mu, int s) {
-  if (mu == 0) kick_link<D, N, R, REP, 0>(a, L, s);
-  else if (mu == 1) kick_link<D, N, R, REP, 1>(a, L, s);
+__device__ __forceinline__ void kick_link_dispatch(const KickArgs& a, const LatDev& L, int mu, int s, const int* x) {
+  if (mu == 0) kick_link<D, N, R, REP, 0>(a, L, s, x);
+  else if (mu == 1) kick_link<D, N, R, REP, 1>(a, L, s, x);
   else if constexpr (D > 2) {
-    if (mu == 2) kick_link<D, N, R, REP, 2>(a, L, s);
-    else if constexpr (D > 3) kick_link<D, N, R, REP, 3>(a, L, s);
+    if (mu == 2) kick_link<D, N, R, REP, 2>(a, L, s, x);
+    else if constexpr (D > 3) kick_link<D, N, R, REP, 3>(a, L, s, x);
   }
 }
 
-// Occupancy: FP32 instances are held to 128 registers (4 blocks of 128 per SM),
-// FP64 instances to 168 (3 blocks).
+// Occupancy: FP32 instances are held to 128 registers (4 blocks of 128 per SM);
+// FP64 instances keep up to 255 (2 blocks): a tighter cap spills.
 template <typename R> struct KickMinBlocks { static constexpr int v = 4; };
-template <> struct KickMinBlocks<double> { static constexpr int v = 3; };
+template <> struct KickMinBlocks<double> { static constexpr int v = 2; };
 
 template <int D, int N, typename R, int REP>
 __global__ void __launch_bounds__(KBLOCK, KickMinBlocks<R>::v) k_kick(const KickArgs a) {
   const Work w = a.work[blockIdx.x];
-  if ((int)threadIdx.x >= w.n) return;
   const LatDev& L = a.lats[w.lat];
-  const int s = w.s0 + threadIdx.x;
-  if (w.mu >= 0) kick_link_dispatch<D, N, R, REP>(a, L, w.mu, s);
-  else if (REP != REP_NONE) kick_site<D, N, R, REP>(a, L, s);
+  int s, x[D];
+  if (!tile_site<D>(L, w, threadIdx.x, s, x)) return;
+  if (w.mu >= 0) kick_link_dispatch<D, N, R, REP>(a, L, w.mu, s, x);
+  else if (REP != REP_NONE) kick_site<D, N, R, REP>(a, L, s, x);
 }
 
 // ---------------------------------------------------------------------------
@@ -473,6 +490,39 @@ __global__ void __launch_bounds__(GEN_WARPS * 32) k_gen_links(const GenArgs a) {
 // exponential and the product in FP64; optional reunitarisation (FP32-MD mode
 // reunitarises every step).  Site items: phi += eps pi (:145-146).
 // ---------------------------------------------------------------------------
+// Projection back to SU(N) after each FP32-MD drift, in FP64: Gram-Schmidt on the
+// first N-1 rows, the last row fixed by det = 1 (SU(2): (-conj u01, conj u00);
+// SU(3): conj(row0 x row1)).  The trajectory-end reunitarisation of the FP64 mode
+// keeps the reference's algorithm (k_reunit).
+template <int N>
+__device__ __forceinline__ void project_su(Mat<N, double>& U) {
+  double n0 = 0.0;
+#pragma unroll
+  for (int j = 0; j < N; ++j) n0 += norm2(U.e[j]);
+  const double i0 = rsqrt(n0);
+#pragma unroll
+  for (int j = 0; j < N; ++j) U.e[j] = scale(U.e[j], i0);
+  if (N == 2) {
+    U.e[2] = mk<double>(-U.e[1].re, U.e[1].im);
+    U.e[3] = mk<double>(U.e[0].re, -U.e[0].im);
+    return;
+  }
+  cx<double> p = zero<double>();
+#pragma unroll
+  for (int j = 0; j < N; ++j) p = add(p, cmul(U.e[j], U.e[N + j]));
+  double n1 = 0.0;
+#pragma unroll
+  for (int j = 0; j < N; ++j) { U.e[N + j] = sub(U.e[N + j], mul(p, U.e[j])); n1 += norm2(U.e[N + j]); }
+  const double i1 = rsqrt(n1);
+#pragma unroll
+  for (int j = 0; j < N; ++j) U.e[N + j] = scale(U.e[N + j], i1);
+  if (N == 3) {
+    U.e[6] = conj(sub(mul(U.e[1], U.e[5]), mul(U.e[2], U.e[4])));
+    U.e[7] = conj(sub(mul(U.e[2], U.e[3]), mul(U.e[0], U.e[5])));
+    U.e[8] = conj(sub(mul(U.e[0], U.e[4]), mul(U.e[1], U.e[3])));
+  }
+}
+
 struct DriftArgs {
   const Work* work;
   const LatDev* lats;
@@ -503,7 +553,7 @@ __global__ void __launch_bounds__(KBLOCK) k_drift(const DriftArgs a) {
     for (int i = 0; i < N * N; ++i) H.e[i] = scale(H.e[i], a.eps);
     const Mat<N, double> E = expi<N>(H);
     Mat<N, double> Un = mm(E, ld_link_rw<N, double>((const R*)a.U, L, mu, s));
-    if (a.reunit) reunitarize<N, double>(Un);
+    if (a.reunit) project_su<N>(Un);
     st_link<N, double>((R*)a.U, L, mu, s, Un);
   } else {
     typedef typename Cmp<R>::t C;

@@ -333,6 +333,21 @@ class Ensemble:
                        ("L_link", "f8")])
         return np.frombuffer(recs, dtype=dt, count=ntraj * self.n_lat).copy().reshape(ntraj, self.n_lat)
 
+    def autotune(self, reps=3):
+        """Pick the kick tile of every group of equal-extent lattices by timing."""
+        ms = C.c_double()
+        self.ctx("gh_autotune", int(reps), C.byref(ms))
+        return ms.value
+
+    def set_tile(self, tile, lat=-1):
+        t = (C.c_int * 4)(*(list(tile) + [1] * (4 - len(tile))))
+        self.ctx("gh_set_tile", lat, t)
+
+    def get_tile(self, lat=0):
+        t = (C.c_int * 4)()
+        self.ctx("gh_get_tile", lat, t)
+        return list(t)[:self.D]
+
     def use_graph(self, on=True):
         self.ctx("gh_use_graph", int(bool(on)))
 

@@ -179,6 +179,16 @@ int gh_read_records(gh_ctx* ctx, int ntraj, gh_traj_record* records);
  * download U, phi and the record.  The drop-in for a driver that keeps the
  * fields in host memory like the reference's GaugeField / CVecField. */
 int gh_trajectory_host(gh_ctx* ctx, double* U, double* phi, gh_traj_record* rec);
+/* ---- kick tiles and the autotuner ----
+ * The kick kernel gives each 128-thread block a 4-D tile of sites (power-of-two
+ * extents per direction); the tile decides how many neighbour links a block
+ * reuses from L1.  gh_autotune times every admissible tile on each group of
+ * equal-extent lattices (reps zero-step kicks each) and keeps the fastest;
+ * best_ms (may be NULL): sum over groups of the best kick time.  Results do not
+ * depend on the tile (every link and site is computed the same way). */
+int gh_autotune(gh_ctx* ctx, int reps, double* best_ms);
+int gh_set_tile(gh_ctx* ctx, int lat, const int* tile);
+int gh_get_tile(gh_ctx* ctx, int lat, int* tile);
 /* Use (1, default) or bypass (0) the captured trajectory graph. */
 int gh_use_graph(gh_ctx* ctx, int enable);
 

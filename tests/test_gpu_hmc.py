@@ -266,3 +266,31 @@ def test_tempering_toggle_and_swaps():
     assert sorted(np.round(kap, 12).tolist()) == sorted(kappas)   # a permutation of the ladder
     for x in (a, b, c):
         x.close()
+
+
+# ---------------------------------------------------------------------------
+# kick tiles: results are independent of the block shape; the autotuner picks one
+# ---------------------------------------------------------------------------
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_kick_tiles_bit_identical(precision):
+    import gauge_higgs_b200 as gh
+    L = [8, 6, 4, 6]
+    h = gh.GaugeHiggsHMC(L, gh.FundamentalRep(3), seed=4, precision=precision, beta=5.7, kappa=0.1, lam=0.5)
+    h.hot(0.8)
+    h.phi_gaussian(12345, 0.3)
+    h.refresh_momenta()
+    P0, pi0 = h.P, h.pi
+    outs = []
+    for tile in ([8, 4, 4, 1], [4, 4, 4, 2], [2, 2, 2, 16], [1, 1, 1, 1], [8, 8, 2, 1]):
+        h.set_tile(tile)
+        assert h.get_tile() == tile
+        h.P = P0
+        h.pi = pi0
+        h.kick(0.05)
+        outs.append((h.P, h.pi))
+    for P, pi in outs[1:]:
+        assert np.array_equal(P, outs[0][0]) and np.array_equal(pi, outs[0][1])
+    ms = h.autotune(reps=2)
+    t = h.get_tile()
+    assert ms > 0 and int(np.prod(t)) <= 128 and all(x & (x - 1) == 0 for x in t)
+    h.close()
