@@ -268,10 +268,11 @@ void default_tile(const int* L, int D, int* lt) {
   for (int mu = 0; mu < D && left > 0; ++mu) { lt[mu] = std::min(left, ceil_log2(L[mu])); left -= lt[mu]; }
 }
 
-// Kick items of the lattices in `lats` (all when empty): for every tile, its D link
-// items (directions of one tile next to each other), then one site item per tile.
+// Kick items of the lattices in `lats`: link items direction by direction (all
+// tiles of direction 0, then direction 1, ...), then one site item per tile.
+// Direction-major order keeps the blocks resident at one time on distinct sites.
 void kick_items(const gh_ctx* ctx, const std::vector<int>& lats, std::vector<Work>& out, int& nlinks, int& nsites) {
-  std::vector<Work> links, sites;
+  std::vector<Work> links, sites, links_mu[4];
   const int D = ctx->D;
   for (int l : lats) {
     const LatDev& Ld = ctx->lat_h[l];
@@ -287,10 +288,11 @@ void kick_items(const gh_ctx* ctx, const std::vector<int>& lats, std::vector<Wor
         s0 += o * Ld.stride[mu];
         packed |= o << (8 * mu);
       }
-      for (int mu = 0; mu < D; ++mu) links.push_back(Work{l, mu, s0, packed});
+      for (int mu = 0; mu < D; ++mu) links_mu[mu].push_back(Work{l, mu, s0, packed});
       sites.push_back(Work{l, -1, s0, packed});
     }
   }
+  for (int mu = 0; mu < D; ++mu) links.insert(links.end(), links_mu[mu].begin(), links_mu[mu].end());
   nlinks = (int)links.size();
   nsites = (int)sites.size();
   out = links;
