@@ -57,11 +57,11 @@ class Dist:
         self.local = int(os.environ.get("LOCAL_RANK", "0"))
         self.pg = None
 
-    def init(self, backend):
+    def init(self, backend, timeout_s=120):
         if self.world > 1:
             import datetime
             import torch.distributed as dist
-            dist.init_process_group(backend, timeout=datetime.timedelta(seconds=120))
+            dist.init_process_group(backend, timeout=datetime.timedelta(seconds=timeout_s))
             self.pg = dist
 
     def barrier(self):
@@ -72,7 +72,8 @@ class Dist:
         if not self.pg:
             return x
         import torch
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dev = "cuda" if self.pg.get_backend() == "nccl" else "cpu"
+        t = torch.tensor([x], dtype=torch.float64, device=dev)
         self.pg.all_reduce(t, op=self.pg.ReduceOp.MAX)
         return float(t.item())
 

@@ -464,11 +464,17 @@ int gh_ctx_create(int D, int N, int n_lat, const int* L, const gh_rep_desc* rep,
   }
   ctx->nU = u; ctx->nP = p; ctx->nF = f; ctx->nG = g;
   std::vector<Work> wg;
-  if (ctx->rep == REP_GEN)
+  int gw = GEN_WARPS;
+  if (ctx->rep == REP_GEN) {
+    // one warp per link holds a tensor buffer of N^n complex numbers in shared memory
+    const size_t per_warp = ((size_t)rep->dimT + 4 * (size_t)rep->d) * 2 * ctx->rs;
+    while (gw > 1 && gw * per_warp > 227 * 1024) gw /= 2;
+    if (per_warp > 227 * 1024) return fail(nullptr, GH_ERR_REP, "general irrep too large for the shared-memory tensor buffer");
     for (int l = 0; l < n_lat; ++l)
       for (int mu = 0; mu < D; ++mu)
-        for (int s0 = 0; s0 < ctx->lat_h[l].V; s0 += GEN_WARPS)
-          wg.push_back(Work{l, mu, s0, std::min(GEN_WARPS, ctx->lat_h[l].V - s0)});
+        for (int s0 = 0; s0 < ctx->lat_h[l].V; s0 += gw)
+          wg.push_back(Work{l, mu, s0, std::min(gw, ctx->lat_h[l].V - s0)});
+  }
   std::vector<Work> wall = wl;
   wall.insert(wall.end(), ws.begin(), ws.end());
 
@@ -494,7 +500,7 @@ int gh_ctx_create(int D, int N, int n_lat, const int* L, const gh_rep_desc* rep,
     if ((rc = build_general(ctx, rep))) { g_err = ctx->err; return rc; }
   }
   b.U = U; b.Us = Us; b.P = P; b.phi = phi; b.phis = phis; b.pi = pi; b.psif = psif; b.psib = psib;
-  b.nw_links = (int)wl.size(); b.nw_sites = (int)ws.size(); b.nw_gen = (int)wg.size();
+  b.nw_links = (int)wl.size(); b.nw_sites = (int)ws.size(); b.nw_gen = (int)wg.size(); b.gen_warps = gw;
   b.hist_cap = 1024;
   b.nlat = n_lat; b.D = D; b.N = N; b.d = ctx->d; b.rep = ctx->rep; b.scalar = ctx->scalar; b.st = ctx->st;
   if ((rc = dalloc(ctx, &b.lats, n_lat)) || (rc = dalloc(ctx, &b.w_all, wall.size())) ||

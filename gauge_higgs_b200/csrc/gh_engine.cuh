@@ -11,8 +11,9 @@ struct Bufs {
   LatDev* lats;
   Work* w_all;     // link items (all lattices, all mu) followed by site items
   int nw_links, nw_sites;
-  Work* w_gen;     // general irrep: items of GEN_WARPS links
+  Work* w_gen;     // general irrep: items of gen_warps links (one warp per link)
   int nw_gen;
+  int gen_warps;   // warps per block of k_gen_links (1..GEN_WARPS, from the tensor size)
   int* blk_first;  // [nlat+1] first site item of each lattice (relative to the site items)
   Work* w_kick;    // kick items over 4-D tiles (LatDev::lt): link items then site items
   int nwk_links, nwk_sites;
@@ -45,7 +46,7 @@ struct Engine : EngineBase {
   typedef typename Cmp<R>::t C;
   Engine() {}
   size_t gen_smem(const Bufs& b) const override {
-    return (size_t)GEN_WARPS * (b.gen.dimT + 4 * b.gen.d) * sizeof(cx<C>);
+    return (size_t)b.gen_warps * (b.gen.dimT + 4 * b.gen.d) * sizeof(cx<C>);
   }
   int prepare(const Bufs& b) override {
     if (REP != REP_GEN) return 0;
@@ -69,7 +70,7 @@ struct Engine : EngineBase {
     a.work = b.w_gen; a.lats = b.lats; a.U = b.U; a.P = b.P; a.phi = b.phi; a.psif = b.psif; a.psib = b.psib;
     a.t = b.gen; a.eps = eps; a.mode = mode; a.out = out;
     const size_t sm = gen_smem(b);
-    k_gen_links<D, N, R><<<b.nw_gen, GEN_WARPS * 32, sm, b.st>>>(a);
+    k_gen_links<D, N, R><<<b.nw_gen, b.gen_warps * 32, sm, b.st>>>(a);
   }
   void drift(const Bufs& b, double eps, int reunit) override {
     DriftArgs a;

@@ -294,3 +294,52 @@ def test_kick_tiles_bit_identical(precision):
     t = h.get_tile()
     assert ms > 0 and int(np.prod(t)) <= 128 and all(x & (x - 1) == 0 for x in t)
     h.close()
+
+
+def test_large_single_row_irrep_su2_spin6():
+    """SU(2) {12} (d = 13, N^n = 4096): the reference's GeneralRep fast-path case
+    (src/rep/rep_general.hpp:161-179).  The engine applies the exact tensor path
+    (fewer warps per block so the 4096-entry buffer fits in shared memory); its
+    forces match the oracle's tensor path and finite differences of the action."""
+    import gauge_higgs_b200 as gh
+    from oracle.oracle import Oracle, REP_GENERAL
+    orc = Oracle()
+    rep = gh.GeneralRep(2, [12])
+    D, N, L = 3, 2, [3, 2, 2]
+    h = gh.GaugeHiggsHMC(L, rep, seed=2, beta=2.3, kappa=0.2, lam=0.5, nmd=6)
+    h.hot(0.6)
+    h.phi_gaussian(3, 0.4)
+    U, phi = h.U, h.phi
+    orep = orc.rep(REP_GENERAL, N, rep.d, 0, rep.n_boxes, rep.dimT, rep.T, rep.W)
+    Fm = orc.matter_force(D, N, L, orep, U, phi, 0.2)
+    Fs = orc.scalar_force(D, N, L, orep, U, phi, 0.2, 0.5)
+    assert np.abs(h.matter_link_force() - Fm).max() < 1e-12 * np.abs(Fm).max()
+    assert np.abs(h.scalar_force() - Fs).max() < 1e-12 * np.abs(Fs).max()
+    assert abs(h.measure()["S_H"] - orc.scalar_action(D, N, L, orep, U, phi, 0.2, 0.5)) < 1e-10
+    h.close()
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_nonfinite_hamiltonian_is_rejected_and_counted(precision):
+    """Failure injected on the host: an overflowing coupling makes H infinite, so
+    dH = inf - inf is NaN.  The device Metropolis step rejects it (every comparison
+    with NaN is false, as in the reference), counts it, and restores the fields;
+    the chain then continues normally."""
+    import gauge_higgs_b200 as gh
+    h = gh.GaugeHiggsHMC([4, 4, 4, 4], gh.FundamentalRep(2), seed=9, precision=precision, beta=2.3, kappa=0.2,
+                         lam=0.5, nmd=8)
+    h.hot(0.5)
+    h.phi_gaussian(12345, 0.3)
+    h.run(2)
+    U0, phi0 = h.U, h.phi
+    h.lam = 1e308
+    dH, acc = gh.Ensemble.trajectory(h)
+    assert np.isnan(dH[0]) and not acc[0]
+    assert np.array_equal(h.U, U0) and np.array_equal(h.phi, phi0)
+    t, a, nonfinite = h.traj_counts(0)
+    assert t == 3 and nonfinite == 1
+    h.lam = 0.5
+    rec = h.run(5)[:, 0]
+    assert np.all(np.isfinite(rec["dH"]))
+    assert h.traj_counts(0)[2] == 1
+    h.close()
