@@ -358,6 +358,131 @@ def run_reference(a, dist):
     }))
 
 
+def run_extra(a, dist):
+    """Additional measurements (not the headline line): the other BASELINE configurations
+    and a lattice larger than L2.  One JSON line per case, rank 0, one GPU."""
+    import torch
+    torch.cuda.set_device(dist.local)
+    import gauge_higgs_b200 as gh
+    from oracle.oracle import Reference, RefSession, have_reference, LEAPFROG, OMELYAN
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+    ref = Reference() if have_reference() else None
+    cores = ref.set_threads(os.cpu_count() or 1) if ref else 0
+
+    def gpu_rate(h, K, W=3):
+        h.set_stream(stream.cuda_stream)
+        h.autotune(reps=2)
+        h.enqueue(W)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        h.enqueue(K)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        rec = h.records(min(K, 1024))
+        return K / (e0.elapsed_time(e1) / 1e3), rec
+
+    def cpu_rate(D, N, L, spec, beta, kappa, lam, nmd, integ, ntraj, phi_sigma=0.3):
+        if ref is None:
+            return None
+        s = RefSession(ref, D, N, L, spec, beta, kappa, lam, nmd, 1.0, 1, integ, 0.8, phi_sigma)
+        t0 = time.perf_counter()
+        s.run(ntraj)
+        dt = time.perf_counter() - t0
+        s.close()
+        return {"value": round(ntraj / dt, 5), "cores": cores, "kind": "reference", "sample": f"{ntraj} trajectories"}
+
+    out = []
+    wl = a.workload
+    if wl in ("c1", "all"):
+        for prec in ("fp64", "fp32"):
+            h = gh.GaugeHiggsHMC([6] * 4, gh.FundamentalRep(2), seed=1, precision=prec, beta=2.3, kappa=0.20, lam=0.5,
+                                 nmd=20, integ="leapfrog")
+            h.hot(0.8)
+            h.phi_gaussian(12345, 0.3)
+            v, rec = gpu_rate(h, 2000)
+            out.append({"workload": "C1 SU(2) fund 6^4 beta=2.3 kappa=0.20 lambda=0.5 leapfrog nmd=20", "precision": prec,
+                        "value": round(v, 1), "unit": "trajectories/s", "acceptance": float(rec["accepted"].mean()),
+                        "cpu_baseline": cpu_rate(4, 2, [6] * 4, "fund", 2.3, 0.2, 0.5, 20, LEAPFROG, 60) if prec == "fp64" else None})
+            h.close()
+    if wl in ("c3", "all"):
+        for spec, rows, real in (("sextet {2}", [2], False), ("octet {2,1}:real", [2, 1], True),
+                                 ("27-plet {4,2}:real", [4, 2], True)):
+            for prec in ("fp64", "fp32"):
+                rep = gh.GeneralRep(3, rows, real=real)
+                h = gh.GaugeHiggsHMC([12] * 4, rep, seed=1, precision=prec, beta=5.7, kappa=0.1, lam=0.5, nmd=20)
+                h.hot(0.8)
+                h.phi_gaussian(12345, 1.0)
+                K = 20 if rows == [4, 2] else 50
+                v, rec = gpu_rate(h, K, W=1)
+                cpu = None
+                if prec == "fp64" and rows != [4, 2]:
+                    sp = ",".join(map(str, rows)) + (":real" if real else "")
+                    cpu = cpu_rate(4, 3, [12] * 4, sp, 5.7, 0.1, 0.5, 20, OMELYAN, 1, phi_sigma=1.0)
+                out.append({"workload": f"C3 SU(3) 12^4 {spec} beta=5.7 kappa=0.1 lambda=0.5 Omelyan nmd=20",
+                            "precision": prec, "value": round(v, 3), "unit": "trajectories/s", "cpu_baseline": cpu})
+                h.close()
+    if wl in ("c4", "all"):
+        Ls = [6, 8, 10, 12]
+        ext = [[L] * 4 for L in Ls for _ in range(16)]
+        kap = [0.22 + 0.006 * i for _ in Ls for i in range(16)]
+        seeds = list(range(1, 65))
+        ens = gh.Ensemble(ext, gh.FundamentalRep(2), seeds=seeds, precision="fp32", beta=2.3, kappa=kap, lam=0.5,
+                          nmd=20, integ="omelyan")
+        ens.hot(0.8)
+        ens.phi_gaussian(12345, 0.3)
+        ens.enable_tempering(True)
+        v, rec = gpu_rate(ens, 100)
+        att, acc, _ = ens.tempering_stats()
+        sites = sum(L ** 4 for L in Ls) * 16
+        cpu = None
+        if ref is not None:
+            t = 0.0
+            for L in Ls:
+                s = RefSession(ref, 4, 2, [L] * 4, "fund", 2.3, 0.25, 0.5, 20, 1.0, 1, OMELYAN, 0.8, 0.3)
+                t0 = time.perf_counter()
+                s.run(2)
+                t += 16 * (time.perf_counter() - t0) / 2
+                s.close()
+            cpu = {"value": round(1.0 / t, 5), "cores": cores, "kind": "reference",
+                   "sample": "2 trajectories of one lattice per L, scaled by 16 lattices per L, run serially"}
+        out.append({"workload": "C4 64 SU(2)+fund lattices (16 each of L=6,8,10,12), beta=2.3 lambda=0.5, kappa grid "
+                                "0.22..0.31, FP32-MD, one graph launch per ensemble trajectory, kappa tempering on",
+                    "value": round(v, 2), "unit": "ensemble trajectories/s (64 lattice trajectories each)",
+                    "site_updates_per_s": round(v * sites * 20 * 2, 1), "acceptance": float(rec["accepted"].mean()),
+                    "swap_acceptance": float(acc.sum() / max(att.sum(), 1)), "cpu_baseline": cpu})
+        ens.close()
+    if wl in ("big", "all"):
+        for prec in ("fp64", "fp32"):
+            L = [32, 32, 32, 32]
+            h = gh.GaugeHiggsHMC(L, gh.FundamentalRep(3), seed=1, precision=prec, beta=5.7, kappa=0.1, lam=0.5, nmd=16)
+            h.set_stream(stream.cuda_stream)
+            h.hot(0.8)
+            h.phi_gaussian(12345, 0.3)
+            h.autotune(reps=2)
+            V = 32 ** 4
+            res = {}
+            for which in ("kick", "drift"):
+                fn = h.kick if which == "kick" else h.drift
+                fn(0.0)
+                torch.cuda.synchronize()
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                for _ in range(10):
+                    fn(0.0)
+                e1.record(stream)
+                torch.cuda.synchronize()
+                ms = e0.elapsed_time(e1) / 10
+                res[which] = {"ms": round(ms, 4), "alg_GBps": round(V * ALG_BYTES[which][prec] / (ms / 1e3) / 1e9, 1)}
+            v, _ = gpu_rate(h, 10, W=1)
+            out.append({"workload": "SU(3) fund 32^4 (1,048,576 sites; fields larger than L2)", "precision": prec,
+                        "value": round(v, 2), "unit": "trajectories/s", "kernels": res, "hbm_peak_GBps": peaks()[0]})
+            h.close()
+    for o in out:
+        print(json.dumps(o))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -366,12 +491,16 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--cpu-traj", type=int, default=3)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--workload", default="c2", choices=["c2", "c1", "c3", "c4", "big", "all"],
+                    help="c2 (default) prints the headline line; the others print additional measurements")
     a = ap.parse_args()
     if a.warmup < 3 and a.impl == "ours":
         a.warmup = 3
     dist = Dist()
     if a.impl == "reference":
         run_reference(a, dist)
+    elif a.workload != "c2":
+        run_extra(a, dist)
     else:
         run_ours(a, dist)
 

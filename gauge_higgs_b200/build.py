@@ -90,12 +90,34 @@ def build(force=False, jobs=None, verbose=False):
         if r.returncode != 0:
             raise RuntimeError(f"link failed: {' '.join(cmd)}\n{r.stdout}\n{r.stderr}")
         os.replace(tmp, LIB)
+    build_drivers(force)
     # drop stale objects of earlier source versions
     keep = set(os.path.basename(o) for o in objs)
     for f in os.listdir(OBJ):
         if f.endswith(".o") and f not in keep:
             os.remove(os.path.join(OBJ, f))
     return LIB
+
+
+DRIVERS = [("hmc_higgs", 4, 2), ("hmc_higgs_su3", 4, 3), ("gh_hmc", 4, 2), ("gh_hmc_su3", 4, 3)]
+
+
+def build_drivers(force=False):
+    """The C++ drivers (drop-in for the reference's hmc_higgs / gh_hmc), one binary per
+    compile-time (NDIM, NCOL) as in the reference build, linked to the library by rpath."""
+    bindir = os.path.join(PKG, "bin")
+    os.makedirs(bindir, exist_ok=True)
+    for name, D, N in DRIVERS:
+        src = os.path.join(PKG, "drivers", name.replace("_su3", "") + ".cpp")
+        out = os.path.join(bindir, name)
+        deps = [src, os.path.join(ROOT, "include", "gauge_higgs_b200.hpp"), LIB]
+        if not force and os.path.exists(out) and os.path.getmtime(out) >= max(os.path.getmtime(d) for d in deps):
+            continue
+        cmd = ["g++", "-O2", "-std=c++17", f"-DNDIM={D}", f"-DNCOL={N}", "-I" + os.path.join(ROOT, "include"), src,
+               "-o", out, "-L" + LIBDIR, "-lgauge_higgs_b200", "-Wl,-rpath,$ORIGIN/../lib"]
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        if r.returncode != 0:
+            raise RuntimeError(f"driver build failed: {' '.join(cmd)}\n{r.stderr}")
 
 
 if __name__ == "__main__":

@@ -1,0 +1,259 @@
+// gauge_higgs_b200.hpp -- C++ host interface over the C ABI (gauge_higgs_b200.h).
+//
+// Mirrors the reference's host-side interface (hlammiv/gauge_higgs) so a driver
+// written against it switches by changing includes and the namespace:
+//   Representation objects   src/rep/representation.hpp:12-32 (FundamentalRep,
+//                            AdjointRep, GeneralRep from Young rows, make_rep spec syntax
+//                            of src/hmc_higgs.cpp:21-34)
+//   GaugeHiggsHMC<D,N>       src/hmc/gauge_higgs_hmc.hpp:15-195: public couplings
+//                            beta/kappa/lambda/tau/nmd/integ, traj_count/accept_count,
+//                            last_dH; kick, drift, md_evolve, hamiltonian,
+//                            refresh_momenta, trajectory, acceptance
+//   GaugeHMC<D,N>            src/hmc/hmc.hpp:12-96 (pure gauge)
+//   observables              avg_plaquette, higgs_length, link_energy, polyakov_loop
+//   Stats                    src/measure/observables.hpp:104-145
+// Fields live on the GPU; U()/phi() copy them to host vectors in the reference's
+// layouts.  Errors throw std::runtime_error, as the reference does.
+#pragma once
+#include <array>
+#include <cmath>
+#include <cstdint>
+#include <sstream>
+#include <stdexcept>
+#include <string>
+#include <vector>
+#include "gauge_higgs_b200.h"
+
+namespace ghb {
+
+inline void check(int rc, const gh_ctx* ctx) {
+  if (rc != GH_OK) throw std::runtime_error(std::string("gauge_higgs_b200: ") + gh_last_error(ctx));
+}
+
+enum class Integrator { Leapfrog, Omelyan2MN };
+enum class Precision { FP64 = GH_PREC_FP64, FP32_MD = GH_PREC_FP32_MD };
+
+// ---- representations ----
+struct Representation {
+  int kind = GH_REP_NONE, N = 0, d = 0, real = 0, n_boxes = 0, nality = 0;
+  long dimT = 0;
+  std::vector<double> T, W;   // complex interleaved (GENERAL only)
+  std::string repname;
+  std::string name() const { return repname; }
+  gh_rep_desc desc() const {
+    gh_rep_desc r{};
+    r.kind = kind; r.d = d; r.real = real; r.n_boxes = n_boxes; r.dimT = dimT;
+    r.T = T.empty() ? nullptr : T.data();
+    r.W = W.empty() ? nullptr : W.data();
+    return r;
+  }
+};
+
+template <int N> Representation FundamentalRep() {
+  Representation r; r.kind = GH_REP_FUND; r.N = N; r.d = N; r.real = 0; r.nality = 1; r.repname = "fundamental"; return r;
+}
+template <int N> Representation AdjointRep() {
+  Representation r; r.kind = GH_REP_ADJ; r.N = N; r.d = N * N - 1; r.real = 1; r.nality = 0; r.repname = "adjoint"; return r;
+}
+// GeneralRep<N>(rows, real): the Young-symmetriser irrep (src/rep/rep_general.hpp:54-84)
+template <int N> Representation GeneralRep(std::vector<int> rows, bool real = false) {
+  Representation r;
+  r.kind = GH_REP_GENERAL; r.N = N; r.real = real ? 1 : 0;
+  long dimT = 0;
+  check(gh_rep_general_info(N, rows.data(), (int)rows.size(), &r.d, &r.n_boxes, &dimT), nullptr);
+  r.dimT = dimT;
+  r.T.assign((size_t)(N * N - 1) * r.d * r.d * 2, 0.0);
+  r.W.assign((size_t)r.d * dimT * 2, 0.0);
+  check(gh_rep_general_build(N, rows.data(), (int)rows.size(), r.T.data(), r.W.data()), nullptr);
+  r.nality = r.n_boxes % N;
+  r.repname = "general[";
+  for (size_t i = 0; i < rows.size(); ++i) r.repname += (i ? "," : "") + std::to_string(rows[i]);
+  r.repname += "]";
+  return r;
+}
+// src/hmc_higgs.cpp:23-34 spec syntax: "fund" | "adj" | "r1,r2,...[:real]"
+template <int N> Representation make_rep(std::string spec) {
+  if (spec == "fund") return FundamentalRep<N>();
+  if (spec == "adj") return AdjointRep<N>();
+  bool real = false;
+  const auto colon = spec.find(':');
+  if (colon != std::string::npos) { real = (spec.substr(colon + 1) == "real"); spec = spec.substr(0, colon); }
+  std::vector<int> rows;
+  std::stringstream ss(spec);
+  std::string tok;
+  while (std::getline(ss, tok, ',')) if (!tok.empty()) rows.push_back(std::atoi(tok.c_str()));
+  if (rows.empty()) throw std::runtime_error("bad rep spec '" + spec + "'");
+  return GeneralRep<N>(rows, real);
+}
+
+// ---- HMC ----
+template <int D, int N>
+class GaugeHiggsHMC {
+ public:
+  // couplings and integrator: public members, as in the reference
+  double beta = 2.3, kappa = 0.1, lambda = 0.5, tau = 1.0;
+  int nmd = 20;
+  Integrator integ = Integrator::Omelyan2MN;
+  std::uint64_t traj_count = 0, accept_count = 0;
+  double last_dH = 0.0;
+  int64_t vol = 1;
+
+  GaugeHiggsHMC(const std::array<int, D>& extents, const Representation& R, std::uint64_t seed,
+                Precision prec = Precision::FP64)
+      : rep_(R), L_(extents) {
+    for (int mu = 0; mu < D; ++mu) vol *= L_[mu];
+    gh_rep_desc desc = rep_.desc();
+    check(gh_ctx_create(D, N, 1, L_.data(), rep_.kind == GH_REP_NONE ? nullptr : &desc, (int)prec, &seed, &ctx_), nullptr);
+  }
+  GaugeHiggsHMC(const GaugeHiggsHMC&) = delete;
+  GaugeHiggsHMC& operator=(const GaugeHiggsHMC&) = delete;
+  ~GaugeHiggsHMC() { gh_ctx_destroy(ctx_); }
+
+  gh_ctx* context() { sync_params(); return ctx_; }
+  const Representation& rep() const { return rep_; }
+
+  // initial fields (src/core/fields.hpp:25-34, src/core/scalar_field.hpp:34-50)
+  void hot(double sigma = 1.0) { check(gh_hot_start(ctx_, sigma), ctx_); }
+  void cold() { check(gh_cold_start(ctx_), ctx_); }
+  void phi_gaussian(std::uint64_t stream, double sigma = 1.0) { check(gh_phi_gaussian(ctx_, stream, sigma), ctx_); }
+  void phi_cold(double c = 1.0) { check(gh_phi_cold(ctx_, c), ctx_); }
+
+  void kick(double eps) { sync_params(); check(gh_kick(ctx_, eps), ctx_); }
+  void drift(double eps) { sync_params(); check(gh_drift(ctx_, eps), ctx_); }
+  void md_evolve() { sync_params(); check(gh_md_evolve(ctx_), ctx_); }
+  void refresh_momenta() { sync_params(); check(gh_refresh_momenta(ctx_), ctx_); }
+  void reunitarize_all() { check(gh_reunitarize(ctx_), ctx_); }
+  double hamiltonian() { return measure().H; }
+
+  bool trajectory() {
+    sync_params();
+    double dH = 0.0;
+    int acc = 0;
+    check(gh_trajectory(ctx_, &dH, &acc), ctx_);
+    last_dH = dH;
+    pull_counters();
+    return acc != 0;
+  }
+  // n trajectories without a host round trip in between; records of each
+  std::vector<gh_traj_record> run(int n) {
+    sync_params();
+    std::vector<gh_traj_record> r((size_t)std::max(n, 0));
+    check(gh_run_trajectories(ctx_, n, r.data()), ctx_);
+    if (n > 0) last_dH = r.back().dH;
+    pull_counters();
+    return r;
+  }
+  double acceptance() const { return traj_count ? double(accept_count) / double(traj_count) : 0.0; }
+
+  gh_obs measure() { sync_params(); gh_obs o; check(gh_measure(ctx_, 0, &o), ctx_); return o; }
+  double avg_plaquette() { return measure().plaquette; }
+  double higgs_length() { return measure().L_phi; }
+  double link_energy() { return measure().L_link; }
+  double polyakov_loop(int tdir = D - 1) { double p; check(gh_polyakov(ctx_, 0, tdir, &p), ctx_); return p; }
+
+  // fields in the reference layouts (complex interleaved doubles)
+  std::vector<double> U() { std::vector<double> u((size_t)vol * D * N * N * 2); check(gh_get_links(ctx_, 0, u.data()), ctx_); return u; }
+  void set_U(const std::vector<double>& u) { check(gh_set_links(ctx_, 0, u.data()), ctx_); }
+  std::vector<double> phi() { std::vector<double> p((size_t)vol * rep_.d * 2); check(gh_get_phi(ctx_, 0, p.data()), ctx_); return p; }
+  void set_phi(const std::vector<double>& p) { check(gh_set_phi(ctx_, 0, p.data()), ctx_); }
+
+  double max_unitarity_violation() {
+    const std::vector<double> u = U();
+    double worst = 0.0;
+    for (size_t l = 0; l < u.size() / (2 * N * N); ++l) {
+      const double* m = &u[l * 2 * N * N];
+      for (int i = 0; i < N; ++i)
+        for (int j = 0; j < N; ++j) {
+          double re = (i == j) ? -1.0 : 0.0, im = 0.0;
+          for (int k = 0; k < N; ++k) {   // (U^dag U)_ij = sum_k conj(U_ki) U_kj
+            const double ar = m[2 * (k * N + i)], ai = -m[2 * (k * N + i) + 1];
+            const double br = m[2 * (k * N + j)], bi = m[2 * (k * N + j) + 1];
+            re += ar * br - ai * bi;
+            im += ar * bi + ai * br;
+          }
+          worst = std::max(worst, std::sqrt(re * re + im * im));
+        }
+    }
+    return worst;
+  }
+
+ protected:
+  void sync_params() {
+    if (beta != pb_ || kappa != pk_ || lambda != pl_) {
+      check(gh_set_couplings(ctx_, 0, beta, kappa, lambda), ctx_);
+      pb_ = beta; pk_ = kappa; pl_ = lambda;
+    }
+    const int ig = integ == Integrator::Leapfrog ? GH_LEAPFROG : GH_OMELYAN;
+    if (tau != pt_ || nmd != pn_ || ig != pi_) {
+      check(gh_set_integrator(ctx_, ig, nmd, tau), ctx_);
+      pt_ = tau; pn_ = nmd; pi_ = ig;
+    }
+    if (traj_count != ptc_ || accept_count != pac_) {
+      check(gh_set_traj_count(ctx_, 0, traj_count, accept_count), ctx_);
+      ptc_ = traj_count; pac_ = accept_count;
+    }
+  }
+  void pull_counters() {
+    std::uint64_t t, a, nf;
+    check(gh_get_traj_count(ctx_, 0, &t, &a, &nf), ctx_);
+    traj_count = ptc_ = t;
+    accept_count = pac_ = a;
+  }
+  Representation rep_;
+  std::array<int, D> L_;
+  gh_ctx* ctx_ = nullptr;
+  double pb_ = NAN, pk_ = NAN, pl_ = NAN, pt_ = NAN;
+  int pn_ = -1, pi_ = -1;
+  std::uint64_t ptc_ = 0, pac_ = 0;
+};
+
+template <int D, int N>
+class GaugeHMC : public GaugeHiggsHMC<D, N> {
+ public:
+  GaugeHMC(const std::array<int, D>& extents, std::uint64_t seed, Precision prec = Precision::FP64)
+      : GaugeHiggsHMC<D, N>(extents, Representation{}, seed, prec) {}
+};
+
+// ---- time-series statistics (src/measure/observables.hpp:104-145) ----
+struct Stats {
+  std::vector<double> x;
+  void add(double v) { x.push_back(v); }
+  int n() const { return (int)x.size(); }
+  double mean() const { double s = 0.0; for (double v : x) s += v; return x.empty() ? 0.0 : s / x.size(); }
+  double var() const {
+    const double m = mean();
+    double s2 = 0.0;
+    for (double v : x) s2 += v * v;
+    return x.empty() ? 0.0 : s2 / x.size() - m * m;
+  }
+  double susceptibility(double volume) const { return volume * var(); }
+  double binder() const {
+    if (x.empty()) return 0.0;
+    const double m = mean();
+    double m2 = 0.0, m4 = 0.0;
+    for (double v : x) { const double d = v - m; m2 += d * d; m4 += d * d * d * d; }
+    m2 /= x.size(); m4 /= x.size();
+    return m2 > 0.0 ? 1.0 - m4 / (3.0 * m2 * m2) : 0.0;
+  }
+  double binned_error(int nbins = 16) const {
+    const int N = n();
+    if (N < 2 * nbins) nbins = std::max(2, N / 2);
+    if (N < 2) return 0.0;
+    const int bs = N / nbins;
+    std::vector<double> bm;
+    for (int b = 0; b < nbins; ++b) {
+      double s = 0.0;
+      for (int i = b * bs; i < (b + 1) * bs; ++i) s += x[i];
+      bm.push_back(s / bs);
+    }
+    double mb = 0.0;
+    for (double v : bm) mb += v;
+    mb /= bm.size();
+    double v = 0.0;
+    for (double b : bm) v += (b - mb) * (b - mb);
+    v /= (bm.size() - 1);
+    return std::sqrt(v / bm.size());
+  }
+};
+
+}  // namespace ghb
