@@ -41,6 +41,7 @@ class TrajRecord(C.Structure):
 
 
 _dp = C.POINTER(C.c_double)
+_fp = C.POINTER(C.c_float)
 _ip = C.POINTER(C.c_int)
 _u64p = C.POINTER(C.c_uint64)
 _ctx = C.c_void_p
@@ -90,6 +91,15 @@ SIGNATURES = {
     "gh_rep_general_info": [C.c_int, _ip, C.c_int, _ip, _ip, C.POINTER(C.c_long)],
     "gh_rep_general_build": [C.c_int, _ip, C.c_int, _dp, _dp],
     "gh_plaquette_noalloc": [C.c_int, C.c_int, _ip, C.c_void_p, C.c_void_p, C.c_void_p],
+    "gh_mlp_create": [C.c_int, _ip, C.c_int, C.c_uint64, C.POINTER(C.c_void_p)],
+    "gh_mlp_destroy": [C.c_void_p],
+    "gh_mlp_num_params": [C.c_void_p, C.POINTER(C.c_long)],
+    "gh_mlp_get_params": [C.c_void_p, _fp],
+    "gh_mlp_set_params": [C.c_void_p, _fp],
+    "gh_mlp_grad": [C.c_void_p, _fp, _fp, C.c_int, _fp, _fp],
+    "gh_mlp_adam_step": [C.c_void_p, C.c_float],
+    "gh_mlp_train": [C.c_void_p, _fp, _fp, C.c_int, C.c_int, C.c_int, C.c_float, C.c_uint64, _fp],
+    "gh_mlp_predict": [C.c_void_p, _fp, C.c_int, _fp, _fp, _fp],
 }
 
 
@@ -108,6 +118,8 @@ def load(path=LIB_PATH):
     lib.gh_rng_uniform.restype = C.c_double
     lib.gh_rng_gauss.argtypes = [C.c_uint64, C.c_uint64]
     lib.gh_rng_gauss.restype = C.c_double
+    lib.gh_mlp_last_error.argtypes = []
+    lib.gh_mlp_last_error.restype = C.c_char_p
     lib.gh_noalloc_last_error.argtypes = []
     lib.gh_noalloc_last_error.restype = C.c_char_p
     lib.gh_last_error.argtypes = [C.c_void_p]

@@ -205,6 +205,32 @@ int gh_temper_enable(gh_ctx* ctx, int mode, uint64_t swap_seed);
  * kappa_of_lat: current kappa of each lattice. */
 int gh_temper_stats(gh_ctx* ctx, uint64_t* attempts, uint64_t* accepts, double* kappa_of_lat);
 
+/* ---- coupling-scan surrogate: an ensemble of MLPs trained on the GPU ----
+ * No counterpart in the reference (its coupling scans are uniform grids of
+ * independent runs, validate_su2higgs.sh / scripts/).  widths: n_layers + 1
+ * layer widths (input first); SiLU between layers; FP32 weights and Adam state,
+ * BF16 hidden activations, FP32 accumulation; loss = mean squared error.
+ * All members see the same minibatches; they differ by initialisation (seed).
+ * Arrays are row-major FP32: x [n][widths[0]], y and outputs [n][widths[n_layers]],
+ * params / grads [member][P] with P = gh_mlp_num_params.  Errors:
+ * gh_mlp_last_error(). */
+typedef struct gh_mlp gh_mlp;
+int gh_mlp_create(int n_members, const int* widths, int n_layers, uint64_t seed, gh_mlp** out);
+int gh_mlp_destroy(gh_mlp* net);
+int gh_mlp_num_params(const gh_mlp* net, long* per_member);
+int gh_mlp_get_params(gh_mlp* net, float* params);
+int gh_mlp_set_params(gh_mlp* net, const float* params);
+/* forward + backward of one batch: grads (may be NULL) and per-member loss (may be NULL) */
+int gh_mlp_grad(gh_mlp* net, const float* x, const float* y, int n, float* grads, float* loss);
+/* one Adam update (beta1 0.9, beta2 0.999, eps 1e-8) from the last gh_mlp_grad */
+int gh_mlp_adam_step(gh_mlp* net, float lr);
+/* epochs of shuffled minibatches; loss: per-member mean loss of the last epoch */
+int gh_mlp_train(gh_mlp* net, const float* x, const float* y, int n, int epochs, int batch, float lr, uint64_t seed,
+                 float* loss);
+/* per_member [M][n][n_out], ensemble mean and variance [n][n_out]; any may be NULL */
+int gh_mlp_predict(gh_mlp* net, const float* x, int n, float* per_member, float* mean, float* var);
+const char* gh_mlp_last_error(void);
+
 /* ---- allocation-free plaquette reduction ----
  * No counterpart in the reference.  For callers that cannot allocate device
  * memory where they measure: a driver recording its own work into a CUDA graph

@@ -25,7 +25,7 @@ def test_library_exports_every_declared_symbol():
     assert not missing, missing
     # the Python binding declares a signature for each of them
     bound = set(_lib.SIGNATURES) | {"gh_last_error", "gh_rng_key", "gh_rng_uniform", "gh_rng_gauss",
-                                      "gh_noalloc_last_error"}
+                                      "gh_noalloc_last_error", "gh_mlp_last_error"}
     assert set(names) <= bound, set(names) - bound
 
 
