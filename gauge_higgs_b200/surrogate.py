@@ -75,30 +75,30 @@ class Surrogate:
         return per * self.ys[None, None, :] + self.ym[None, None, :]    # [members, n, 3]
 
     def kappa_c(self, L, lo, hi, beta=2.3, lam=0.5, h=5e-4):
-        """Per member: argmax of d<L_link>/dkappa on a fine grid; returns (mean, spread, per-member)."""
+        """Per member: argmax of d<L_link>/dkappa on a fine grid.  Returns the median over
+        members (robust to a stray member), the spread (std) and the per-member values."""
         grid = np.arange(lo, hi + h / 2, h)
         ll = self.predict(grid, np.full(len(grid), L), beta, lam)[:, :, 0]
         dll = np.gradient(ll, grid, axis=1)
         kc = grid[np.argmax(dll, axis=1)]
-        return float(kc.mean()), float(kc.std()), kc
+        return float(np.median(kc)), float(kc.std()), kc
 
     def close(self):
         self.net.close()
 
 
-def locate_kappa_c(L, lo=0.18, hi=0.34, n_init=5, rounds=3, per_round=4, ntherm=100, nmeas=300, beta=2.3, lam=0.5,
+def locate_kappa_c(L, lo=0.18, hi=0.34, n_init=5, rounds=3, per_round=4, ntherm=60, nmeas=150, beta=2.3, lam=0.5,
                    nmd=12, precision="fp32", seed=100):
     """Active learning: a coarse grid, then rounds of points placed where the ensemble
-    members disagree about kappa_c.  Returns (kappa_c, spread, trajectories, points)."""
+    members disagree about kappa_c (the consensus and its spread, never narrower than
+    +-0.004).  Returns (kappa_c, spread, trajectories, points)."""
     pts, cost = scan(np.linspace(lo, hi, n_init), L, ntherm, nmeas, beta, lam, nmd, precision, seed)
     sur = Surrogate(seed=seed)
     for r in range(rounds):
         sur.fit(pts, beta, lam)
         kc, sd, per = sur.kappa_c(L, lo, hi, beta, lam)
-        # new points: the members' kappa_c estimates and their spread around the consensus
-        width = max(2.5 * sd, 0.004)
-        cand = np.linspace(kc - width, kc + width, per_round)
-        cand = np.clip(cand, lo, hi)
+        width = max(2.0 * sd, 0.004)
+        cand = np.clip(np.linspace(kc - width, kc + width, per_round), lo, hi)
         new, c = scan(cand, L, ntherm, nmeas, beta, lam, nmd, precision, seed + 97 * (r + 1))
         cost += c
         pts = {k: np.concatenate([pts[k], new[k]]) for k in pts}
