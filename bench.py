@@ -479,6 +479,37 @@ def run_extra(a, dist):
             out.append({"workload": "SU(3) fund 32^4 (1,048,576 sites; fields larger than L2)", "precision": prec,
                         "value": round(v, 2), "unit": "trajectories/s", "kernels": res, "hbm_peak_GBps": peaks()[0]})
             h.close()
+    if wl in ("validate", "all"):
+        # FP32-MD against FP64 at equal couplings: thermalise, then n trajectories each; means
+        # with 16-bin jackknife errors (src/measure/observables.hpp:129-144)
+        from gauge_higgs_b200.stats import Stats
+        n, ntherm = a.validate_traj, 200
+        res = {}
+        for prec in ("fp64", "fp32"):
+            h = gh.GaugeHiggsHMC(WL["L"], gh.FundamentalRep(3), seed=77, precision=prec, beta=WL["beta"],
+                                 kappa=WL["kappa"], lam=WL["lam"], nmd=WL["nmd"], tau=WL["tau"], integ=WL["integ"])
+            h.set_stream(stream.cuda_stream)
+            h.hot(WL["hot_sigma"])
+            h.phi_gaussian(12345, WL["phi_sigma"])
+            h.run(ntherm, records=False)
+            recs = []
+            for t0 in range(0, n, 1000):
+                recs.append(h.run(min(1000, n - t0))[:, 0])
+            rec = np.concatenate(recs)
+            r = {}
+            for k in ("plaquette", "L_phi", "L_link", "accepted"):
+                st = Stats(rec[k].astype(float))
+                r[k] = (st.mean(), st.binned_error())
+            st = Stats(np.exp(-rec["dH"]))
+            r["exp_minus_dH"] = (st.mean(), st.binned_error())
+            res[prec] = r
+            h.close()
+        delta = {k: round((res["fp32"][k][0] - res["fp64"][k][0]) /
+                          max(np.hypot(res["fp32"][k][1], res["fp64"][k][1]), 1e-300), 2) for k in res["fp64"]}
+        out.append({"workload": f"validate: FP32-MD vs FP64, {WORKLOAD}, {ntherm} thermalisation + {n} trajectories each",
+                    "fp64": {k: [round(v[0], 6), round(v[1], 6)] for k, v in res["fp64"].items()},
+                    "fp32": {k: [round(v[0], 6), round(v[1], 6)] for k, v in res["fp32"].items()},
+                    "difference_in_combined_sigma": delta})
     for o in out:
         print(json.dumps(o))
 
@@ -491,7 +522,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--cpu-traj", type=int, default=3)
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--workload", default="c2", choices=["c2", "c1", "c3", "c4", "big", "all"],
+    ap.add_argument("--validate-traj", type=int, default=2000)
+    ap.add_argument("--workload", default="c2", choices=["c2", "c1", "c3", "c4", "big", "validate", "all"],
                     help="c2 (default) prints the headline line; the others print additional measurements")
     a = ap.parse_args()
     if a.warmup < 3 and a.impl == "ours":
