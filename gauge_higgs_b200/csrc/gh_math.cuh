@@ -261,10 +261,20 @@ template <int N> GH_HD Mat<N, double> expi(const Mat<N, double>& H) {
 // c0 = det Q for traceless Q): Q^n = a_n I + b_n Q + g_n Q^2 with
 // (a, b, g)_{n+1} = (c0 g_n, a_n + c1 g_n, b_n).  The series runs on three
 // scalars instead of 3x3 matrices; exp(iQ) = f0 I + f1 Q + f2 Q^2.
+// 1/n for the series coefficients (multiplications instead of FP64 divisions)
+GH_HD double inv_int(int n) {
+  switch (n) {
+    case 1: return 1.0; case 2: return 0.5; case 3: return 1.0 / 3.0; case 4: return 0.25; case 5: return 0.2;
+    case 6: return 1.0 / 6.0; case 7: return 1.0 / 7.0; case 8: return 0.125; case 9: return 1.0 / 9.0;
+    case 10: return 0.1; case 11: return 1.0 / 11.0; case 12: return 1.0 / 12.0; case 13: return 1.0 / 13.0;
+    case 14: return 1.0 / 14.0; case 15: return 1.0 / 15.0; case 16: return 0.0625; case 17: return 1.0 / 17.0;
+    case 18: return 1.0 / 18.0; case 19: return 1.0 / 19.0; case 20: return 0.05; default: return 1.0 / n;
+  }
+}
 template <> GH_HD Mat<3, double> expi<3>(const Mat<3, double>& H) {
-  double nrm = sqrt(fnorm2(H));
+  double nrm2 = fnorm2(H);          // scale until ||H||_F / 2^s <= 1/2, compared squared
   int s = 0;
-  while (nrm > 0.5) { nrm *= 0.5; ++s; }
+  while (nrm2 > 0.25) { nrm2 *= 0.25; ++s; }
   const double sc = ldexp(1.0, -s);
   Mat<3, double> Q;
 #pragma unroll
@@ -277,7 +287,7 @@ template <> GH_HD Mat<3, double> expi<3>(const Mat<3, double>& H) {
   for (int n = 1; n <= 40; ++n) {
     const double an = c0 * g, bn = a + c1 * g, gn = b;
     a = an; b = bn; g = gn;
-    coef /= n;
+    coef *= inv_int(n);
     const double ta = coef * a, tb = coef * b, tg = coef * g;
     switch (n & 3) {   // i^n = 1, i, -1, -i
       case 0: f0r += ta; f1r += tb; f2r += tg; break;
