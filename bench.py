@@ -483,7 +483,7 @@ def run_extra(a, dist):
         # FP32-MD against FP64 at equal couplings: thermalise, then n trajectories each; means
         # with 16-bin jackknife errors (src/measure/observables.hpp:129-144)
         from gauge_higgs_b200.stats import Stats
-        n, ntherm = a.validate_traj, 200
+        n, ntherm = a.validate_traj, a.validate_therm
         res = {}
         for prec in ("fp64", "fp32"):
             h = gh.GaugeHiggsHMC(WL["L"], gh.FundamentalRep(3), seed=77, precision=prec, beta=WL["beta"],
@@ -523,6 +523,7 @@ def main():
     ap.add_argument("--cpu-traj", type=int, default=3)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--validate-traj", type=int, default=2000)
+    ap.add_argument("--validate-therm", type=int, default=200)
     ap.add_argument("--workload", default="c2", choices=["c2", "c1", "c3", "c4", "big", "validate", "all"],
                     help="c2 (default) prints the headline line; the others print additional measurements")
     a = ap.parse_args()

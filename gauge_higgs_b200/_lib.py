@@ -37,7 +37,12 @@ class Obs(C.Structure):
 
 class TrajRecord(C.Structure):
     _fields_ = [("dH", C.c_double), ("accepted", C.c_int), ("traj", C.c_int), ("plaquette", C.c_double),
-                ("L_phi", C.c_double), ("L_link", C.c_double)]
+                ("L_phi", C.c_double), ("L_link", C.c_double), ("kappa", C.c_double)]
+
+
+# numpy view of an array of TrajRecord
+TRAJ_DTYPE = [("dH", "f8"), ("accepted", "i4"), ("traj", "i4"), ("plaquette", "f8"), ("L_phi", "f8"),
+              ("L_link", "f8"), ("kappa", "f8")]
 
 
 _dp = C.POINTER(C.c_double)

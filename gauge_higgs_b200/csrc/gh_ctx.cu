@@ -260,10 +260,10 @@ int xfer_field(gh_ctx* ctx, int lat, int kind, void* dev, const double* host, bo
 
 int ceil_log2(int x) { int k = 0; while ((1 << k) < x) ++k; return k; }
 
-// Default kick tile: fill the 7 bits of a 128-thread block direction by direction
-// (direction 0 first), never wider than the lattice -- the shape of 128 consecutive sites.
+// Default kick tile: fill the KICK_LOG2 bits of a kick block direction by direction
+// (direction 0 first), never wider than the lattice -- the shape of consecutive sites.
 void default_tile(const int* L, int D, int* lt) {
-  int left = 7;
+  int left = KICK_LOG2;
   for (int mu = 0; mu < 4; ++mu) lt[mu] = 0;
   for (int mu = 0; mu < D && left > 0; ++mu) { lt[mu] = std::min(left, ceil_log2(L[mu])); left -= lt[mu]; }
 }
@@ -786,7 +786,7 @@ int gh_set_tile(gh_ctx* ctx, int lat, const int* tile) {
     lt[mu] = ceil_log2(tile[mu]);
     sum += lt[mu];
   }
-  if (sum > 7) return fail(ctx, GH_ERR_ARG, "a tile holds at most 128 sites");
+  if (sum > KICK_LOG2) return fail(ctx, GH_ERR_ARG, "a tile holds at most as many sites as a kick block has threads");
   const int l0 = lat < 0 ? 0 : lat, l1 = lat < 0 ? ctx->nlat : lat + 1;
   for (int l = l0; l < l1; ++l) std::memcpy(ctx->lat_h[l].lt, lt, sizeof(lt));
   return rebuild_kick_table(ctx);
@@ -801,7 +801,7 @@ int gh_get_tile(gh_ctx* ctx, int lat, int* tile) {
 }
 
 // Choose the kick tile of every group of equal-extent lattices by timing: each
-// admissible shape (power-of-two extents, 128 sites, no wider than the lattice)
+// admissible shape (power-of-two extents, KICK_BLOCK sites, no wider than the lattice)
 // runs `reps` zero-step kicks on that group alone; the fastest is kept.
 int gh_autotune(gh_ctx* ctx, int reps, double* best_ms) {
   if (!ctx) return fail(nullptr, GH_ERR_ARG, "null context");
@@ -818,8 +818,8 @@ int gh_autotune(gh_ctx* ctx, int reps, double* best_ms) {
     const std::vector<int>& ext = kv.first;
     const std::vector<int>& lats = kv.second;
     int maxb[4] = {0, 0, 0, 0}, summax = 0;
-    for (int mu = 0; mu < ctx->D; ++mu) { maxb[mu] = std::min(7, ceil_log2(ext[mu])); summax += maxb[mu]; }
-    const int target = std::min(7, summax);
+    for (int mu = 0; mu < ctx->D; ++mu) { maxb[mu] = std::min(KICK_LOG2, ceil_log2(ext[mu])); summax += maxb[mu]; }
+    const int target = std::min(KICK_LOG2, summax);
     double best = 1e30;
     int best_lt[4] = {0, 0, 0, 0};
     int lt[4] = {0, 0, 0, 0};
@@ -896,7 +896,7 @@ int gh_run_trajectories(gh_ctx* ctx, int ntraj, gh_traj_record* records) {
           const unsigned long long tr = L[l].traj - (unsigned long long)(nt - t);   // traj number - 1 of record t
           const TrajRec& r = h[(size_t)l * cap + (int)(tr % (unsigned long long)cap)];
           gh_traj_record& o = records[(size_t)(t0 + t) * ctx->nlat + l];
-          o.dH = r.dH; o.accepted = r.accepted; o.traj = r.traj; o.plaquette = r.plaq; o.L_phi = r.L_phi; o.L_link = r.L_link;
+          o.dH = r.dH; o.accepted = r.accepted; o.traj = r.traj; o.plaquette = r.plaq; o.L_phi = r.L_phi; o.L_link = r.L_link; o.kappa = r.kappa;
         }
     }
   }
@@ -926,7 +926,7 @@ int gh_read_records(gh_ctx* ctx, int ntraj, gh_traj_record* records) {
       if (L[l].traj < (unsigned long long)(ntraj - t)) { std::memset(&o, 0, sizeof(o)); continue; }
       const unsigned long long tr = L[l].traj - (unsigned long long)(ntraj - t);
       const TrajRec& r = h[(size_t)l * cap + (int)(tr % (unsigned long long)cap)];
-      o.dH = r.dH; o.accepted = r.accepted; o.traj = r.traj; o.plaquette = r.plaq; o.L_phi = r.L_phi; o.L_link = r.L_link;
+      o.dH = r.dH; o.accepted = r.accepted; o.traj = r.traj; o.plaquette = r.plaq; o.L_phi = r.L_phi; o.L_link = r.L_link; o.kappa = r.kappa;
     }
   return GH_OK;
 }
@@ -948,6 +948,7 @@ int gh_trajectory_host(gh_ctx* ctx, double* U, double* phi, gh_traj_record* rec)
     const int slot = (int)((L.traj - 1) % (unsigned long long)ctx->b.hist_cap);
     CK(cudaMemcpy(&r, ctx->b.hist + slot, sizeof(r), cudaMemcpyDeviceToHost));
     rec->dH = r.dH; rec->accepted = r.accepted; rec->traj = r.traj; rec->plaquette = r.plaq; rec->L_phi = r.L_phi; rec->L_link = r.L_link;
+    rec->kappa = r.kappa;
   } else {
     CK(cudaStreamSynchronize(ctx->st));
   }

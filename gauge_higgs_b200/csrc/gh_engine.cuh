@@ -62,7 +62,7 @@ struct Engine : EngineBase {
     const int count = (links ? b.nwk_links : 0) + (do_sites ? b.nwk_sites : 0);
     if (count == 0) return;
     a.work = b.w_kick + first;
-    k_kick<D, N, R, REP><<<count, KBLOCK, 0, b.st>>>(a);
+    k_kick<D, N, R, REP><<<count, KICK_BLOCK, 0, b.st>>>(a);
   }
   void gen_links(const Bufs& b, double eps, int mode, double* out) override {
     if (REP != REP_GEN) return;

@@ -23,6 +23,11 @@ enum { REP_NONE = 0, REP_FUND = 1, REP_ADJ = 2, REP_GEN = 3 };
 enum { F_GAUGE = 1, F_MATTER = 2 };
 enum { M_UPDATE = 0, M_WRITE = 1 };
 constexpr int KBLOCK = 128;    // threads per block of site/link kernels
+#ifndef GH_KICK_LOG2
+#define GH_KICK_LOG2 7
+#endif
+constexpr int KICK_LOG2 = GH_KICK_LOG2;      // sites per kick tile (= threads per kick block), log2
+constexpr int KICK_BLOCK = 1 << KICK_LOG2;
 constexpr int GEN_WARPS = 4;   // warps per block of the general-irrep kernel
 constexpr int NRED = 6;        // per-site partial sums of the measure kernel
 
@@ -342,11 +347,11 @@ __device__ __forceinline__ void kick_link_dispatch(const KickArgs& a, const LatD
 
 // Occupancy: FP32 instances are held to 128 registers (4 blocks of 128 per SM);
 // FP64 instances keep up to 255 (2 blocks): a tighter cap spills.
-template <typename R> struct KickMinBlocks { static constexpr int v = 4; };
-template <> struct KickMinBlocks<double> { static constexpr int v = 2; };
+template <typename R> struct KickMinBlocks { static constexpr int v = 4 * 128 / KICK_BLOCK; };
+template <> struct KickMinBlocks<double> { static constexpr int v = 2 * 128 / KICK_BLOCK > 0 ? 2 * 128 / KICK_BLOCK : 1; };
 
 template <int D, int N, typename R, int REP>
-__global__ void __launch_bounds__(KBLOCK, KickMinBlocks<R>::v) k_kick(const KickArgs a) {
+__global__ void __launch_bounds__(KICK_BLOCK, KickMinBlocks<R>::v) k_kick(const KickArgs a) {
   const Work w = a.work[blockIdx.x];
   const LatDev& L = a.lats[w.lat];
   int s, x[D];
@@ -754,7 +759,7 @@ static __global__ void k_finalize(const FinArgs a) {
 // uniform(key(0xE5 | 0xB2, traj)); NaN/Inf dH rejects (as in the reference,
 // where every comparison with NaN is false) and is counted.  Appends a record.
 // ---------------------------------------------------------------------------
-struct TrajRec { double dH; int accepted; int traj; double plaq, L_phi, L_link; };
+struct TrajRec { double dH; int accepted; int traj; double plaq, L_phi, L_link, kappa; };
 struct MetroArgs { LatDev* lats; const double* res; TrajRec* hist; int hist_cap; int nlat; int pure; };
 static __global__ void k_metropolis(const MetroArgs a) {
   const int l = blockIdx.x * blockDim.x + threadIdx.x;
@@ -779,6 +784,7 @@ static __global__ void k_metropolis(const MetroArgs a) {
     h.plaq = ro[5];
     h.L_phi = ro[7];
     h.L_link = ro[6];
+    h.kappa = L.kappa;
   }
 }
 

@@ -17,7 +17,7 @@ import ctypes as C
 import numpy as np
 
 from . import _lib
-from ._lib import LIB, check, GaugeHiggsError, RepDesc, Obs, TrajRecord
+from ._lib import LIB, check, GaugeHiggsError, RepDesc, Obs, TrajRecord, TRAJ_DTYPE
 
 LEAPFROG, OMELYAN = _lib.LEAPFROG, _lib.OMELYAN
 _INTEG = {"leapfrog": LEAPFROG, "omelyan": OMELYAN, LEAPFROG: LEAPFROG, OMELYAN: OMELYAN}
@@ -316,8 +316,7 @@ class Ensemble:
             return None
         recs = (TrajRecord * (ntraj * self.n_lat))()
         self.ctx("gh_run_trajectories", int(ntraj), recs)
-        dt = np.dtype([("dH", "f8"), ("accepted", "i4"), ("traj", "i4"), ("plaquette", "f8"), ("L_phi", "f8"),
-                       ("L_link", "f8")])
+        dt = np.dtype(TRAJ_DTYPE)
         arr = np.frombuffer(recs, dtype=dt, count=ntraj * self.n_lat).copy()
         return arr.reshape(ntraj, self.n_lat)
 
@@ -329,8 +328,7 @@ class Ensemble:
         """Records of the last ntraj (<= 1024) trajectories, [ntraj, n_lat]."""
         recs = (TrajRecord * (ntraj * self.n_lat))()
         self.ctx("gh_read_records", int(ntraj), recs)
-        dt = np.dtype([("dH", "f8"), ("accepted", "i4"), ("traj", "i4"), ("plaquette", "f8"), ("L_phi", "f8"),
-                       ("L_link", "f8")])
+        dt = np.dtype(TRAJ_DTYPE)
         return np.frombuffer(recs, dtype=dt, count=ntraj * self.n_lat).copy().reshape(ntraj, self.n_lat)
 
     def autotune(self, reps=3):

@@ -70,12 +70,14 @@ typedef struct {
 } gh_obs;
 
 /* One trajectory of one lattice: dH, accept, and the driver's measurements
- * after accept/reject (src/hmc_higgs.cpp:80-87). */
+ * after accept/reject (src/hmc_higgs.cpp:80-87); kappa is the hopping parameter
+ * the trajectory ran at (it moves between lattices under kappa tempering). */
 typedef struct {
   double dH;
   int accepted;
   int traj;
   double plaquette, L_phi, L_link;
+  double kappa;
 } gh_traj_record;
 
 typedef struct gh_ctx gh_ctx;
