@@ -139,9 +139,9 @@ template <int N, typename C>
 __device__ __forceinline__ void fund_apply(const Mat<N, C>& U, const cx<C>* v, cx<C>* o, bool dag) {
 #pragma unroll
   for (int i = 0; i < N; ++i) {
-    cx<C> s = dag ? cmul(U.e[i], v[0]) : mul(U.e[i * N], v[0]);
+    cx<C> s = zero<C>();
 #pragma unroll
-    for (int j = 1; j < N; ++j) s = add(s, dag ? cmul(U.e[j * N + i], v[j]) : mul(U.e[i * N + j], v[j]));
+    for (int j = 0; j < N; ++j) s = dag ? cfma_cj(s, U.e[j * N + i], v[j]) : cfma(s, U.e[i * N + j], v[j]);
     o[i] = s;
   }
 }
@@ -201,16 +201,9 @@ __device__ __forceinline__ void kick_link(const KickArgs& a, const LatDev& L, in
       const int spn = nfwd(L, s, x[nu], nu);
       const int smn = nbwd(L, s, x[nu], nu);
       const int spm_mn = nbwd(L, spm, x[nu], nu);
-      {
-        Mat<N, C> A = mm_nd(ld_link<N, C>(U, L, nu, spm), ld_link<N, C>(U, L, mu, spn));
-        A = mm_nd(A, ld_link<N, C>(U, L, nu, s));
-        acc(sig, A);
-      }
-      {
-        Mat<N, C> B = mm_dd(ld_link<N, C>(U, L, nu, spm_mn), ld_link<N, C>(U, L, mu, smn));
-        B = mm(B, ld_link<N, C>(U, L, nu, smn));
-        acc(sig, B);
-      }
+      // upper staple U_nu(x+mu) U_mu(x+nu)^dag U_nu(x)^dag, lower U_nu(x+mu-nu)^dag U_mu(x-nu)^dag U_nu(x-nu)
+      mm_nd_acc(sig, mm_nd(ld_link<N, C>(U, L, nu, spm), ld_link<N, C>(U, L, mu, spn)), ld_link<N, C>(U, L, nu, s));
+      mm_acc(sig, mm_dd(ld_link<N, C>(U, L, nu, spm_mn), ld_link<N, C>(U, L, mu, smn)), ld_link<N, C>(U, L, nu, smn));
     }
     Om = mm(Umu, sig);
     const C c = (C)(L.beta / N);
@@ -393,7 +386,7 @@ __device__ void gen_apply(const GenTables& t, const Mat<N, C>& M, bool dag, cons
     cx<C> s = zero<C>();
     for (int p = t.wt_ptr[i]; p < t.wt_ptr[i + 1]; ++p) {
       const double2 w = t.wt_v[p];
-      s = add(s, mul(vin[t.wt_l[p]], mk<C>((C)w.x, (C)w.y)));
+      s = cfma(s, vin[t.wt_l[p]], mk<C>((C)w.x, (C)w.y));
     }
     buf[i] = s;
   }
@@ -409,9 +402,9 @@ __device__ void gen_apply(const GenTables& t, const Mat<N, C>& M, bool dag, cons
       for (int j = 0; j < N; ++j) v[j] = buf[base + j * blk];
 #pragma unroll
       for (int j = 0; j < N; ++j) {
-        cx<C> s = dag ? cmul(M.e[j], v[0]) : mul(M.e[j * N], v[0]);
+        cx<C> s = zero<C>();
 #pragma unroll
-        for (int g = 1; g < N; ++g) s = add(s, dag ? cmul(M.e[g * N + j], v[g]) : mul(M.e[j * N + g], v[g]));
+        for (int g = 0; g < N; ++g) s = dag ? cfma_cj(s, M.e[g * N + j], v[g]) : cfma(s, M.e[j * N + g], v[g]);
         buf[base + j * blk] = s;
       }
     }
@@ -422,7 +415,7 @@ __device__ void gen_apply(const GenTables& t, const Mat<N, C>& M, bool dag, cons
     cx<C> s = zero<C>();
     for (int p = t.w_ptr[k]; p < t.w_ptr[k + 1]; ++p) {
       const double2 w = t.w_v[p];
-      s = add(s, cmul(mk<C>((C)w.x, (C)w.y), buf[t.w_i[p]]));
+      s = cfma_cj(s, mk<C>((C)w.x, (C)w.y), buf[t.w_i[p]]);
     }
     vout[k] = s;
   }
@@ -475,9 +468,9 @@ __global__ void __launch_bounds__(GEN_WARPS * 32) k_gen_links(const GenArgs a) {
       const int r = g * d + i;
       for (int p = a.t.t_ptr[r]; p < a.t.t_ptr[r + 1]; ++p) {
         const double2 tv = a.t.t_v[p];
-        ti = add(ti, mul(mk<C>((C)tv.x, (C)tv.y), pf[a.t.t_j[p]]));
+        ti = cfma(ti, mk<C>((C)tv.x, (C)tv.y), pf[a.t.t_j[p]]);
       }
-      z = add(z, cmul(px[i], ti));
+      z = cfma_cj(z, px[i], ti);
     }
     const C F = -(C)L.kappa * (C(-2) * z.im);
     const long long pi_ = L.p_off + ((long long)mu * ng + g) * L.V + s;

@@ -55,58 +55,96 @@ template <int N, typename T> GH_HD void acc(Mat<N, T>& A, const Mat<N, T>& B) {
   for (int i = 0; i < N * N; ++i) A.e[i] = add(A.e[i], B.e[i]);
 }
 
-// C = A B ; C = A B^dag ; C = A^dag B ; C = A^dag B^dag   (sum over k in order 0..N-1)
-template <int N, typename T> GH_HD Mat<N, T> mm(const Mat<N, T>& A, const Mat<N, T>& B) {
-  Mat<N, T> C;
+// Fused multiply-add, rounded once, on host and device alike.
+GH_HD float fmad(float a, float b, float c) {
+#if defined(__CUDA_ARCH__)
+  return __fmaf_rn(a, b, c);
+#else
+  return fmaf(a, b, c);
+#endif
+}
+GH_HD double fmad(double a, double b, double c) {
+#if defined(__CUDA_ARCH__)
+  return __fma_rn(a, b, c);
+#else
+  return fma(a, b, c);
+#endif
+}
+
+// s + a b and s + conj(a) b as four fused multiply-adds each
+template <typename T> GH_HD cx<T> cfma(cx<T> s, cx<T> a, cx<T> b) {
+  s.re = fmad(a.re, b.re, s.re);
+  s.re = fmad(-a.im, b.im, s.re);
+  s.im = fmad(a.re, b.im, s.im);
+  s.im = fmad(a.im, b.re, s.im);
+  return s;
+}
+template <typename T> GH_HD cx<T> cfma_cj(cx<T> s, cx<T> a, cx<T> b) {
+  s.re = fmad(a.re, b.re, s.re);
+  s.re = fmad(a.im, b.im, s.re);
+  s.im = fmad(a.re, b.im, s.im);
+  s.im = fmad(-a.im, b.re, s.im);
+  return s;
+}
+
+// Matrix products C (+)= op(A) op(B), op = identity or dagger (DA, DB).  Every
+// output entry is one chain of fused multiply-adds over k = 0..N-1: a complex
+// multiply-accumulate is 4 FMAs (re += ar br -/+ ai bi, im += ar bi +/- ai br, the
+// conjugation signs folded into operand negations), where the written-out form
+// s + (ar br - ai bi) costs 6 (one product of each pair cannot fuse).
+template <int N, typename T, bool DA, bool DB, bool ACC>
+GH_HD void mm_core(const Mat<N, T>& A, const Mat<N, T>& B, Mat<N, T>& C) {
 #pragma unroll
   for (int i = 0; i < N; ++i)
 #pragma unroll
     for (int j = 0; j < N; ++j) {
-      cx<T> s = mul(A.e[i * N], B.e[j]);
+      cx<T> s = ACC ? C.e[i * N + j] : zero<T>();
 #pragma unroll
-      for (int k = 1; k < N; ++k) s = add(s, mul(A.e[i * N + k], B.e[k * N + j]));
+      for (int k = 0; k < N; ++k) {
+        const cx<T> a = DA ? A.e[k * N + i] : A.e[i * N + k];
+        const cx<T> b = DB ? B.e[j * N + k] : B.e[k * N + j];
+        const T ai = DA ? -a.im : a.im;       // im of op(A)_ik
+        const T bi = DB ? -b.im : b.im;       // im of op(B)_kj
+        if (!ACC && k == 0) {
+          s.re = a.re * b.re;
+          s.im = a.re * bi;
+        } else {
+          s.re = fmad(a.re, b.re, s.re);
+          s.im = fmad(a.re, bi, s.im);
+        }
+        s.re = fmad(-ai, bi, s.re);
+        s.im = fmad(ai, b.re, s.im);
+      }
       C.e[i * N + j] = s;
     }
+}
+// C = A B ; C = A B^dag ; C = A^dag B ; C = A^dag B^dag
+template <int N, typename T> GH_HD Mat<N, T> mm(const Mat<N, T>& A, const Mat<N, T>& B) {
+  Mat<N, T> C;
+  mm_core<N, T, false, false, false>(A, B, C);
   return C;
 }
 template <int N, typename T> GH_HD Mat<N, T> mm_nd(const Mat<N, T>& A, const Mat<N, T>& B) {
   Mat<N, T> C;
-#pragma unroll
-  for (int i = 0; i < N; ++i)
-#pragma unroll
-    for (int j = 0; j < N; ++j) {
-      cx<T> s = mulc(A.e[i * N], B.e[j * N]);
-#pragma unroll
-      for (int k = 1; k < N; ++k) s = add(s, mulc(A.e[i * N + k], B.e[j * N + k]));
-      C.e[i * N + j] = s;
-    }
+  mm_core<N, T, false, true, false>(A, B, C);
   return C;
 }
 template <int N, typename T> GH_HD Mat<N, T> mm_dn(const Mat<N, T>& A, const Mat<N, T>& B) {
   Mat<N, T> C;
-#pragma unroll
-  for (int i = 0; i < N; ++i)
-#pragma unroll
-    for (int j = 0; j < N; ++j) {
-      cx<T> s = cmul(A.e[i], B.e[j]);
-#pragma unroll
-      for (int k = 1; k < N; ++k) s = add(s, cmul(A.e[k * N + i], B.e[k * N + j]));
-      C.e[i * N + j] = s;
-    }
+  mm_core<N, T, true, false, false>(A, B, C);
   return C;
 }
 template <int N, typename T> GH_HD Mat<N, T> mm_dd(const Mat<N, T>& A, const Mat<N, T>& B) {
   Mat<N, T> C;
-#pragma unroll
-  for (int i = 0; i < N; ++i)
-#pragma unroll
-    for (int j = 0; j < N; ++j) {
-      cx<T> s = cmulc(A.e[i], B.e[j * N]);
-#pragma unroll
-      for (int k = 1; k < N; ++k) s = add(s, cmulc(A.e[k * N + i], B.e[j * N + k]));
-      C.e[i * N + j] = s;
-    }
+  mm_core<N, T, true, true, false>(A, B, C);
   return C;
+}
+// C += A B ; C += A B^dag
+template <int N, typename T> GH_HD void mm_acc(Mat<N, T>& C, const Mat<N, T>& A, const Mat<N, T>& B) {
+  mm_core<N, T, false, false, true>(A, B, C);
+}
+template <int N, typename T> GH_HD void mm_nd_acc(Mat<N, T>& C, const Mat<N, T>& A, const Mat<N, T>& B) {
+  mm_core<N, T, false, true, true>(A, B, C);
 }
 // Re Tr(A B^dag) = sum_ij Re(A_ij conj(B_ij))
 template <int N, typename T> GH_HD T retr_nd(const Mat<N, T>& A, const Mat<N, T>& B) {
