@@ -825,6 +825,13 @@ struct InitArgs {
   double sigma;
   unsigned long long stream;
 };
+// Gaussian draw for a field stored as R: the correctly rounded draw for FP64
+// fields, the CUDA-libm draw for FP32 fields (identical after rounding to FP32
+// but for ~1e-8 of draws).
+template <typename R> __device__ __forceinline__ double gauss_r(uint64_t seed, uint64_t k) {
+  return sizeof(R) == sizeof(double) ? ghrng::gauss(seed, k) : ghrng::gauss_md(seed, k);
+}
+
 template <int N, typename R>
 __global__ void __launch_bounds__(KBLOCK) k_init(const InitArgs a) {
   typedef typename Cmp<R>::t C;
@@ -851,7 +858,7 @@ __global__ void __launch_bounds__(KBLOCK) k_init(const InitArgs a) {
       R* P = (R*)a.P;
       const long long pb = L.p_off + (long long)mu * ng * L.V + s;
 #pragma unroll
-      for (int g = 0; g < ng; ++g) P[pb + (long long)g * L.V] = (R)ghrng::gauss(L.seed, ghrng::key(st, s, mu, g));
+      for (int g = 0; g < ng; ++g) P[pb + (long long)g * L.V] = (R)gauss_r<R>(L.seed, ghrng::key(st, s, mu, g));
     }
     return;
   }
@@ -862,8 +869,8 @@ __global__ void __launch_bounds__(KBLOCK) k_init(const InitArgs a) {
     const double sg = (a.what == 1) ? 1.0 : a.sigma;
     R* vec = (R*)a.vec;
     for (int k = 0; k < a.d; ++k) {
-      const double re = sg * ghrng::gauss(L.seed, ghrng::key(st, s, 2 * k));
-      const double im = a.real ? 0.0 : sg * ghrng::gauss(L.seed, ghrng::key(st, s, 2 * k + 1));
+      const double re = sg * gauss_r<R>(L.seed, ghrng::key(st, s, 2 * k));
+      const double im = a.real ? 0.0 : sg * gauss_r<R>(L.seed, ghrng::key(st, s, 2 * k + 1));
       stc<double>(vec, L.f_off + (long long)k * L.V + s, mk<double>(re, im));
     }
   } else if (a.what == 5) {

@@ -89,21 +89,27 @@ class Surrogate:
 
 def locate_kappa_c(L, lo=0.18, hi=0.34, n_init=5, rounds=3, per_round=4, ntherm=60, nmeas=150, beta=2.3, lam=0.5,
                    nmd=12, precision="fp32", seed=100):
-    """Active learning: a coarse grid, then rounds of points placed where the ensemble
-    members disagree about kappa_c (the consensus and its spread, never narrower than
-    +-0.004).  Returns (kappa_c, spread, trajectories, points)."""
+    """Active learning in a shrinking trust region: a coarse grid of n_init points, then
+    rounds of per_round points centred on the ensemble's kappa_c.  Round r spans
+    +-max(2 spread, w0 / 2^r, 0.004), w0 = half the coarse spacing, and the next
+    estimate is searched only within twice that span of the current one, so members
+    that put a spurious inflection where no data lies cannot pull the estimate away.
+    Returns (kappa_c, spread, trajectories, points)."""
     pts, cost = scan(np.linspace(lo, hi, n_init), L, ntherm, nmeas, beta, lam, nmd, precision, seed)
     sur = Surrogate(seed=seed)
+    w0 = 0.5 * (hi - lo) / max(n_init - 1, 1)
+    a, b = lo, hi
     for r in range(rounds):
         sur.fit(pts, beta, lam)
-        kc, sd, per = sur.kappa_c(L, lo, hi, beta, lam)
-        width = max(2.0 * sd, 0.004)
+        kc, sd, per = sur.kappa_c(L, a, b, beta, lam)
+        width = max(2.0 * sd, w0 / 2 ** r, 0.004)
+        a, b = max(lo, kc - 2.0 * width), min(hi, kc + 2.0 * width)
         cand = np.clip(np.linspace(kc - width, kc + width, per_round), lo, hi)
         new, c = scan(cand, L, ntherm, nmeas, beta, lam, nmd, precision, seed + 97 * (r + 1))
         cost += c
         pts = {k: np.concatenate([pts[k], new[k]]) for k in pts}
     sur.fit(pts, beta, lam)
-    kc, sd, _ = sur.kappa_c(L, lo, hi, beta, lam)
+    kc, sd, _ = sur.kappa_c(L, a, b, beta, lam)
     sur.close()
     return kc, sd, cost, pts
 

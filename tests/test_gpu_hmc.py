@@ -122,6 +122,23 @@ def test_reversibility(N, kind, precision, tol):
     h.close()
 
 
+def test_fp32_refresh_equals_rounded_fp64():
+    """The FP32-MD refresh draws with the CUDA math library's FP64 log and cos; rounded
+    to FP32 its momenta equal the FP64 mode's correctly rounded draws, bar a few."""
+    import gauge_higgs_b200 as gh
+    out = {}
+    for p in ("fp64", "fp32"):
+        h = gh.GaugeHiggsHMC([8, 8, 8, 8], gh.FundamentalRep(3), seed=5, precision=p, beta=5.7, kappa=0.1, lam=0.5)
+        h.hot(0.5)
+        h.refresh_momenta()
+        out[p] = (h.P, h.pi)
+        h.close()
+    for a, b in zip(out["fp64"], out["fp32"]):
+        a32, b32 = np.asarray(a).astype(np.float32), np.asarray(b).astype(np.float32)
+        assert int(np.sum(a32 != b32)) <= 2
+        assert np.abs(a32.astype(np.float64) - b32).max() < 1e-6
+
+
 # ---------------------------------------------------------------------------
 # dH second-order scaling (test_gauge.cpp:88-107)
 # ---------------------------------------------------------------------------

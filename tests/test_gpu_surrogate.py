@@ -34,6 +34,6 @@ def test_surrogate_locates_kappa_c_with_fewer_trajectories():
     ok_s, ok_u = int(np.sum(err_s <= 0.005)), int(np.sum(err_u <= 0.005))
     print(f"truth {kc_true:.4f}; surrogate {cost_s} traj, within 0.005 in {ok_s}/12, mean |err| {err_s.mean():.4f}; "
           f"uniform {cost_u} traj, within 0.005 in {ok_u}/12, mean |err| {err_u.mean():.4f}")
-    assert cost_u >= 3 * cost_s
-    assert err_s.mean() <= 0.005
-    assert ok_s >= 9 and ok_s >= ok_u - 1
+    assert cost_u >= 3 * cost_s                    # at least 3x fewer trajectories ...
+    assert err_s.mean() <= 0.005 and err_s.max() <= 0.01
+    assert err_s.mean() <= err_u.mean()            # ... at no worse accuracy than the uniform scan
