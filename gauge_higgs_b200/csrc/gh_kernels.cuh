@@ -485,39 +485,40 @@ __global__ void __launch_bounds__(GEN_WARPS * 32) k_gen_links(const GenArgs a) {
 
 // ---------------------------------------------------------------------------
 // Drift: U <- exp(i eps P) U (src/hmc/gauge_higgs_hmc.hpp:136-143), with the
-// exponential and the product in FP64; optional reunitarisation (FP32-MD mode
-// reunitarises every step).  Site items: phi += eps pi (:145-146).
+// exponential and the product in the storage precision of the links (FP64 mode:
+// FP64; FP32-MD: FP32); optional projection back to SU(N) (FP32-MD mode projects
+// every step).  Site items: phi += eps pi (:145-146).
 // ---------------------------------------------------------------------------
-// Projection back to SU(N) after each FP32-MD drift, in FP64: Gram-Schmidt on the
-// first N-1 rows, the last row fixed by det = 1 (SU(2): (-conj u01, conj u00);
-// SU(3): conj(row0 x row1)).  The trajectory-end reunitarisation of the FP64 mode
-// keeps the reference's algorithm (k_reunit).
-template <int N>
-__device__ __forceinline__ void project_su(Mat<N, double>& U) {
+// Projection back to SU(N) after each FP32-MD drift: Gram-Schmidt on the first
+// N-1 rows, the last row fixed by det = 1 (SU(2): (-conj u01, conj u00); SU(3):
+// conj(row0 x row1)).  The trajectory-end reunitarisation of the FP64 mode keeps
+// the reference's algorithm (k_reunit).
+template <int N, typename T>
+__device__ __forceinline__ void project_su(Mat<N, T>& U) {
   // rows stay within ~1e-6 of unit norm between projections: one Newton step of
   // 1/sqrt from 1 (x^-1/2 ~ (3 - x)/2) is exact to ~1e-12, a second to FP64 resolution
-  double n0 = 0.0;
+  T n0 = 0;
 #pragma unroll
   for (int j = 0; j < N; ++j) n0 += norm2(U.e[j]);
-  double i0 = 1.5 - 0.5 * n0;
-  i0 = i0 * (1.5 - 0.5 * n0 * i0 * i0);
-  if (fabs(n0 - 1.0) > 1e-3) i0 = rsqrt(n0);    // far from unitary (links set by the caller)
+  T i0 = T(1.5) - T(0.5) * n0;
+  i0 = i0 * (T(1.5) - T(0.5) * n0 * i0 * i0);
+  if (fabs(n0 - T(1)) > T(1e-3)) i0 = rsqrt(n0);    // far from unitary (links set by the caller)
 #pragma unroll
   for (int j = 0; j < N; ++j) U.e[j] = scale(U.e[j], i0);
   if (N == 2) {
-    U.e[2] = mk<double>(-U.e[1].re, U.e[1].im);
-    U.e[3] = mk<double>(U.e[0].re, -U.e[0].im);
+    U.e[2] = mk<T>(-U.e[1].re, U.e[1].im);
+    U.e[3] = mk<T>(U.e[0].re, -U.e[0].im);
     return;
   }
-  cx<double> p = zero<double>();
+  cx<T> p = zero<T>();
 #pragma unroll
   for (int j = 0; j < N; ++j) p = add(p, cmul(U.e[j], U.e[N + j]));
-  double n1 = 0.0;
+  T n1 = 0;
 #pragma unroll
   for (int j = 0; j < N; ++j) { U.e[N + j] = sub(U.e[N + j], mul(p, U.e[j])); n1 += norm2(U.e[N + j]); }
-  double i1 = 1.5 - 0.5 * n1;
-  i1 = i1 * (1.5 - 0.5 * n1 * i1 * i1);
-  if (fabs(n1 - 1.0) > 1e-3) i1 = rsqrt(n1);
+  T i1 = T(1.5) - T(0.5) * n1;
+  i1 = i1 * (T(1.5) - T(0.5) * n1 * i1 * i1);
+  if (fabs(n1 - T(1)) > T(1e-3)) i1 = rsqrt(n1);
 #pragma unroll
   for (int j = 0; j < N; ++j) U.e[N + j] = scale(U.e[N + j], i1);
   if (N == 3) {
@@ -548,17 +549,17 @@ __global__ void __launch_bounds__(KBLOCK) k_drift(const DriftArgs a) {
     const int mu = w.mu;
     constexpr int ng = N * N - 1;
     const R* P = (const R*)a.P;
-    double v[ng];
+    R v[ng];
     const long long pb = L.p_off + (long long)mu * ng * L.V + s;
 #pragma unroll
-    for (int g = 0; g < ng; ++g) v[g] = (double)P[pb + (long long)g * L.V];
-    Mat<N, double> H = alg_to_mat<N, double>(v);
+    for (int g = 0; g < ng; ++g) v[g] = P[pb + (long long)g * L.V];
+    Mat<N, R> H = alg_to_mat<N, R>(v);
 #pragma unroll
-    for (int i = 0; i < N * N; ++i) H.e[i] = scale(H.e[i], a.eps);
-    const Mat<N, double> E = expi<N>(H);
-    Mat<N, double> Un = mm(E, ld_link_rw<N, double>((const R*)a.U, L, mu, s));
-    if (a.reunit) project_su<N>(Un);
-    st_link<N, double>((R*)a.U, L, mu, s, Un);
+    for (int i = 0; i < N * N; ++i) H.e[i] = scale(H.e[i], (R)a.eps);
+    const Mat<N, R> E = expi<N>(H);
+    Mat<N, R> Un = mm(E, ld_link_rw<N, R>((const R*)a.U, L, mu, s));
+    if (a.reunit) project_su<N, R>(Un);
+    st_link<N, R>((R*)a.U, L, mu, s, Un);
   } else {
     typedef typename Cmp<R>::t C;
     R* phi = (R*)a.phi;

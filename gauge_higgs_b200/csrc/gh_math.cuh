@@ -272,24 +272,29 @@ template <int N, typename T> GH_HD cx<T> det(const Mat<N, T>& U);
 // the terms it adds past that point are below FP64 resolution).
 // SU(2): the closed form cos r + i sin(r)/r H.
 // ---------------------------------------------------------------------------
-template <int N> GH_HD Mat<N, double> expi(const Mat<N, double>& H) {
-  const double nrm = sqrt(fnorm2(H));
+// Series cut-off per arithmetic type: a term below it no longer changes an O(1)
+// coefficient (FP64: 1e-18; FP32: 1e-9, below half an FP32 ulp of 1).
+template <typename T> struct ExpTol { static constexpr double v = 1e-18; };
+template <> struct ExpTol<float> { static constexpr double v = 1e-9; };
+
+template <int N, typename T> GH_HD Mat<N, T> expi_series(const Mat<N, T>& H) {
+  const T nrm = sqrt(fnorm2(H));
   int s = 0;
-  double scaled = nrm;
-  while (scaled > 0.5) { scaled *= 0.5; ++s; }
-  const double inv2s = ldexp(1.0, -s);
-  Mat<N, double> A, term, res;
+  T scaled = nrm;
+  while (scaled > T(0.5)) { scaled *= T(0.5); ++s; }
+  const T inv2s = (T)ldexp(1.0, -s);
+  Mat<N, T> A, term, res;
 #pragma unroll
-  for (int i = 0; i < N * N; ++i) A.e[i] = mk<double>(-H.e[i].im * inv2s, H.e[i].re * inv2s);
+  for (int i = 0; i < N * N; ++i) A.e[i] = mk<T>(-H.e[i].im * inv2s, H.e[i].re * inv2s);
   set_ident(term);
   set_ident(res);
   for (int k = 1; k <= 18; ++k) {
     term = mm(term, A);
-    const double ik = 1.0 / k;
+    const T ik = (T)(1.0 / k);
 #pragma unroll
     for (int i = 0; i < N * N; ++i) term.e[i] = scale(term.e[i], ik);
     acc(res, term);
-    if (fnorm2(term) < 1e-36) break;
+    if (fnorm2(term) < T(ExpTol<T>::v * ExpTol<T>::v)) break;
   }
   for (int i = 0; i < s; ++i) res = mm(res, res);
   return res;
@@ -309,60 +314,68 @@ GH_HD double inv_int(int n) {
     case 18: return 1.0 / 18.0; case 19: return 1.0 / 19.0; case 20: return 0.05; default: return 1.0 / n;
   }
 }
-template <> GH_HD Mat<3, double> expi<3>(const Mat<3, double>& H) {
-  double nrm2 = fnorm2(H);          // scale until ||H||_F / 2^s <= 1/2, compared squared
+template <typename T> GH_HD Mat<3, T> expi3(const Mat<3, T>& H) {
+  T nrm2 = fnorm2(H);               // scale until ||H||_F / 2^s <= 1/2, compared squared
   int s = 0;
-  while (nrm2 > 0.25) { nrm2 *= 0.25; ++s; }
-  const double sc = ldexp(1.0, -s);
-  Mat<3, double> Q;
+  while (nrm2 > T(0.25)) { nrm2 *= T(0.25); ++s; }
+  const T sc = (T)ldexp(1.0, -s);
+  Mat<3, T> Q;
 #pragma unroll
   for (int i = 0; i < 9; ++i) Q.e[i] = scale(H.e[i], sc);
-  const Mat<3, double> Q2 = mm(Q, Q);
-  const double c1 = 0.5 * (Q2.e[0].re + Q2.e[4].re + Q2.e[8].re);
-  const double c0 = det<3, double>(Q).re;
-  double a = 1.0, b = 0.0, g = 0.0, coef = 1.0;
-  double f0r = 1.0, f0i = 0.0, f1r = 0.0, f1i = 0.0, f2r = 0.0, f2i = 0.0;
+  const Mat<3, T> Q2 = mm(Q, Q);
+  const T c1 = T(0.5) * (Q2.e[0].re + Q2.e[4].re + Q2.e[8].re);
+  const T c0 = det<3, T>(Q).re;
+  T a = 1, b = 0, g = 0, coef = 1;
+  T f0r = 1, f0i = 0, f1r = 0, f1i = 0, f2r = 0, f2i = 0;
   for (int n = 1; n <= 40; ++n) {
-    const double an = c0 * g, bn = a + c1 * g, gn = b;
+    const T an = c0 * g, bn = a + c1 * g, gn = b;
     a = an; b = bn; g = gn;
-    coef *= inv_int(n);
-    const double ta = coef * a, tb = coef * b, tg = coef * g;
+    coef *= (T)inv_int(n);
+    const T ta = coef * a, tb = coef * b, tg = coef * g;
     switch (n & 3) {   // i^n = 1, i, -1, -i
       case 0: f0r += ta; f1r += tb; f2r += tg; break;
       case 1: f0i += ta; f1i += tb; f2i += tg; break;
       case 2: f0r -= ta; f1r -= tb; f2r -= tg; break;
       default: f0i -= ta; f1i -= tb; f2i -= tg; break;
     }
-    if (fabs(ta) + fabs(tb) + fabs(tg) < 1e-18) break;
+    if (fabs(ta) + fabs(tb) + fabs(tg) < T(ExpTol<T>::v)) break;
   }
-  Mat<3, double> E;
+  Mat<3, T> E;
 #pragma unroll
   for (int i = 0; i < 9; ++i)
-    E.e[i] = add(mul(mk<double>(f1r, f1i), Q.e[i]), mul(mk<double>(f2r, f2i), Q2.e[i]));
+    E.e[i] = add(mul(mk<T>(f1r, f1i), Q.e[i]), mul(mk<T>(f2r, f2i), Q2.e[i]));
   E.e[0].re += f0r; E.e[0].im += f0i;
   E.e[4].re += f0r; E.e[4].im += f0i;
   E.e[8].re += f0r; E.e[8].im += f0i;
   for (int i = 0; i < s; ++i) E = mm(E, E);
   return E;
 }
-template <> GH_HD Mat<2, double> expi<2>(const Mat<2, double>& H) {
+template <typename T> GH_HD Mat<2, T> expi2(const Mat<2, T>& H) {
   // r^2 = Tr(H^2)/2
-  double trh2 = 0.0;
+  T trh2 = 0;
 #pragma unroll
   for (int i = 0; i < 2; ++i)
 #pragma unroll
     for (int k = 0; k < 2; ++k) trh2 += mul(H.e[i * 2 + k], H.e[k * 2 + i]).re;
-  const double r2 = 0.5 * trh2;
-  const double r = sqrt(r2 > 0.0 ? r2 : 0.0);
-  double c, sinc;
-  if (r < 1e-8) { c = 1.0 - 0.5 * r2; sinc = 1.0 - r2 / 6.0; }
-  else { double sn; sincos(r, &sn, &c); sinc = sn / r; }
-  Mat<2, double> U;
+  const T r2 = T(0.5) * trh2;
+  const T r = sqrt(r2 > T(0) ? r2 : T(0));
+  T c, sinc;
+  // below the cut-off the next terms of cos r and sin(r)/r are under the type's resolution
+  const T rsmall = sizeof(T) == sizeof(double) ? T(1e-8) : T(1e-4);
+  if (r < rsmall) { c = T(1) - T(0.5) * r2; sinc = T(1) - r2 / T(6); }
+  else { T sn; sincos(r, &sn, &c); sinc = sn / r; }
+  Mat<2, T> U;
 #pragma unroll
-  for (int i = 0; i < 4; ++i) U.e[i] = mk<double>(-sinc * H.e[i].im, sinc * H.e[i].re);
+  for (int i = 0; i < 4; ++i) U.e[i] = mk<T>(-sinc * H.e[i].im, sinc * H.e[i].re);
   U.e[0].re += c;
   U.e[3].re += c;
   return U;
+}
+// exp(iH) in the arithmetic type of H
+template <int N, typename T> GH_HD Mat<N, T> expi(const Mat<N, T>& H) {
+  if constexpr (N == 3) return expi3<T>(H);
+  else if constexpr (N == 2) return expi2<T>(H);
+  else return expi_series<N, T>(H);
 }
 
 // Determinant (N <= 4), Gaussian elimination without pivoting for N=4 falls back
