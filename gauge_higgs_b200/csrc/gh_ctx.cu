@@ -447,14 +447,14 @@ int gh_ctx_create(int D, int N, int n_lat, const int* L, const gh_rep_desc* rep,
       if (L[l * D + mu] < 1) return fail(nullptr, GH_ERR_ARG, "lattice extents must be >= 1");
       Ld.L[mu] = L[l * D + mu]; Ld.stride[mu] = (int)V; V *= L[l * D + mu];
     }
-    if (V * D * N * N > (1LL << 31) - 1) return fail(nullptr, GH_ERR_ARG, "lattice too large for 32-bit site indexing");
-    Ld.V = (int)V; Ld.cidx = l;
+    if ((V + ULANE) * D * N * N > (1LL << 31) - 1) return fail(nullptr, GH_ERR_ARG, "lattice too large for 32-bit site indexing");
+    Ld.V = (int)V; Ld.Vp = (int)((V + ULANE - 1) / ULANE * ULANE); Ld.cidx = l;
     Ld.u_off = u; Ld.p_off = p; Ld.f_off = f; Ld.g_off = g;
     Ld.beta = 2.3; Ld.kappa = 0.1; Ld.lambda = 0.5; Ld.seed = seeds[l];
     for (int mu = 0; mu < D; ++mu)
       if (L[l * D + mu] > 256) return fail(nullptr, GH_ERR_UNSUPPORTED, "lattice extents above 256 are not supported");
     default_tile(L + l * D, D, Ld.lt);
-    u += V * D * N * N; p += V * D * ctx->ng; f += V * ctx->d; g += (ctx->rep == REP_GEN) ? V * D * ctx->d : 0;
+    u += (long long)Ld.Vp * D * N * N; p += V * D * ctx->ng; f += V * ctx->d; g += (ctx->rep == REP_GEN) ? V * D * ctx->d : 0;
     ctx->lat_h.push_back(Ld);
     for (int mu = 0; mu < D; ++mu)
       for (int s0 = 0; s0 < V; s0 += KBLOCK) wl.push_back(Work{l, mu, s0, (int)std::min<long long>(KBLOCK, V - s0)});

@@ -1,9 +1,13 @@
 // gh_kernels.cuh -- sm_100a kernels of the gauge + Higgs molecular-dynamics path.
 //
-// Device layout (component-major SoA, one plane per matrix/vector component so
-// a warp's load of one component for 32 consecutive sites is one 512 B (FP64)
-// or 256 B (FP32) coalesced transaction; complex = {re,im} vector load):
-//   U   [lat][mu][i*N+j][site]   complex R     (reference: [site*D+mu] N x N, src/core/fields.hpp:12-20)
+// Device layout (component-major, so that a warp's load of one component for 32
+// consecutive sites is one 512 B (FP64) or 256 B (FP32) coalesced transaction;
+// complex = {re,im} vector load):
+//   U   [lat][mu][site/32][i*N+j][site%32]  complex R  (reference: [site*D+mu] N x N, src/core/fields.hpp:12-20)
+//        blocks of 32 sites, the N*N components of a block side by side: the
+//        components of one link lie at a fixed stride of 32 elements, so one
+//        address serves all N*N loads (immediate offsets); the volume is padded
+//        to a multiple of 32 (LatDev::Vp)
 //   P   [lat][mu][a][site]       real R        (reference: [site*D+mu][a], src/core/fields.hpp:46-57)
 //   phi [lat][k][site]           complex R     (reference: [site*d+k], src/core/scalar_field.hpp:15)
 // R = double (FP64 mode) or float (FP32-MD mode).  Several lattices of unequal
@@ -30,11 +34,13 @@ constexpr int KICK_LOG2 = GH_KICK_LOG2;      // sites per kick tile (= threads p
 constexpr int KICK_BLOCK = 1 << KICK_LOG2;
 constexpr int GEN_WARPS = 4;   // warps per block of the general-irrep kernel
 constexpr int NRED = 6;        // per-site partial sums of the measure kernel
+constexpr int ULANE = 32;      // sites per block of the link-field layout
 
 struct LatDev {
   int L[4];
   int stride[4];
   int V;
+  int Vp;                        // V rounded up to a multiple of ULANE (link-field plane size)
   int cidx;                      // coupling index (tempering bookkeeping)
   long long u_off, p_off, f_off, g_off;  // complex / real / complex / complex element offsets
   double beta, kappa, lambda;
@@ -75,27 +81,31 @@ template <typename C, typename R> __device__ __forceinline__ void stc(R* p, long
   v.y = (R)z.im;
   reinterpret_cast<typename V2<R>::t*>(p)[i] = v;
 }
+// Element index of component c of link (mu, s); component c + k sits k * ULANE further on.
+__device__ __forceinline__ long long u_index(const LatDev& L, int nn, int mu, int c, int s) {
+  return L.u_off + (long long)mu * nn * L.Vp + ((long long)(s / ULANE) * nn + c) * ULANE + (s % ULANE);
+}
 template <int N, typename C, typename R>
 __device__ __forceinline__ Mat<N, C> ld_link(const R* __restrict__ U, const LatDev& L, int mu, int s) {
   Mat<N, C> M;
-  const long long base = L.u_off + (long long)mu * N * N * L.V + s;
+  const long long base = u_index(L, N * N, mu, 0, s);
 #pragma unroll
-  for (int c = 0; c < N * N; ++c) M.e[c] = ldc<C>(U, base + (long long)c * L.V);
+  for (int c = 0; c < N * N; ++c) M.e[c] = ldc<C>(U, base + c * ULANE);
   return M;
 }
 template <int N, typename C, typename R>
 __device__ __forceinline__ Mat<N, C> ld_link_rw(const R* U, const LatDev& L, int mu, int s) {
   Mat<N, C> M;
-  const long long base = L.u_off + (long long)mu * N * N * L.V + s;
+  const long long base = u_index(L, N * N, mu, 0, s);
 #pragma unroll
-  for (int c = 0; c < N * N; ++c) M.e[c] = ldc_rw<C>(U, base + (long long)c * L.V);
+  for (int c = 0; c < N * N; ++c) M.e[c] = ldc_rw<C>(U, base + c * ULANE);
   return M;
 }
 template <int N, typename C, typename R>
 __device__ __forceinline__ void st_link(R* U, const LatDev& L, int mu, int s, const Mat<N, C>& M) {
-  const long long base = L.u_off + (long long)mu * N * N * L.V + s;
+  const long long base = u_index(L, N * N, mu, 0, s);
 #pragma unroll
-  for (int c = 0; c < N * N; ++c) stc<C>(U, base + (long long)c * L.V, M.e[c]);
+  for (int c = 0; c < N * N; ++c) stc<C>(U, base + c * ULANE, M.e[c]);
 }
 
 template <int D> __device__ __forceinline__ void coords(const LatDev& L, int s, int* x) {
@@ -794,8 +804,8 @@ __global__ void __launch_bounds__(KBLOCK) k_restore(const RestoreArgs a) {
   typedef typename V2<R>::t V;
   if (w.mu >= 0) {
     const int NN = a.N * a.N;
-    const long long b = L.u_off + (long long)w.mu * NN * L.V + s;
-    for (int c = 0; c < NN; ++c) reinterpret_cast<V*>(a.U)[b + (long long)c * L.V] = reinterpret_cast<const V*>(a.Us)[b + (long long)c * L.V];
+    const long long b = u_index(L, NN, w.mu, 0, s);
+    for (int c = 0; c < NN; ++c) reinterpret_cast<V*>(a.U)[b + c * ULANE] = reinterpret_cast<const V*>(a.Us)[b + c * ULANE];
   } else {
     for (int k = 0; k < a.d; ++k) {
       const long long i = L.f_off + (long long)k * L.V + s;
@@ -936,7 +946,8 @@ __global__ void k_xfer(const XferArgs a) {
       R* P = (R*)a.dev;
       if (a.to_dev) P[di] = (R)a.host_aos[e]; else a.host_aos[e] = (double)P[di];
     } else {
-      const long long di = ((a.kind == 0) ? L.u_off : L.f_off) + (long long)r * L.V + s;  // r = mu*NN + c or k
+      // r = mu*NN + c (links) or k (vectors)
+      const long long di = (a.kind == 0) ? u_index(L, a.ncomp, r / a.ncomp, r % a.ncomp, s) : L.f_off + (long long)r * L.V + s;
       if (a.to_dev) stc<double>((R*)a.dev, di, mk<double>(a.host_aos[2 * e], a.host_aos[2 * e + 1]));
       else { const cx<double> z = ldc_rw<double>((const R*)a.dev, di); a.host_aos[2 * e] = z.re; a.host_aos[2 * e + 1] = z.im; }
     }
