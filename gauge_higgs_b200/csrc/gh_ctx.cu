@@ -454,7 +454,8 @@ int gh_ctx_create(int D, int N, int n_lat, const int* L, const gh_rep_desc* rep,
     for (int mu = 0; mu < D; ++mu)
       if (L[l * D + mu] > 256) return fail(nullptr, GH_ERR_UNSUPPORTED, "lattice extents above 256 are not supported");
     default_tile(L + l * D, D, Ld.lt);
-    u += (long long)Ld.Vp * D * N * N; p += V * D * ctx->ng; f += V * ctx->d; g += (ctx->rep == REP_GEN) ? V * D * ctx->d : 0;
+    u += (long long)Ld.Vp * D * N * N; p += (long long)Ld.Vp * D * ctx->ng; f += (long long)Ld.Vp * ctx->d;
+    g += (ctx->rep == REP_GEN) ? (long long)Ld.Vp * D * ctx->d : 0;
     ctx->lat_h.push_back(Ld);
     for (int mu = 0; mu < D; ++mu)
       for (int s0 = 0; s0 < V; s0 += KBLOCK) wl.push_back(Work{l, mu, s0, (int)std::min<long long>(KBLOCK, V - s0)});

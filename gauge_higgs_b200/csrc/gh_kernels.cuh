@@ -8,8 +8,8 @@
 //        components of one link lie at a fixed stride of 32 elements, so one
 //        address serves all N*N loads (immediate offsets); the volume is padded
 //        to a multiple of 32 (LatDev::Vp)
-//   P   [lat][mu][a][site]       real R        (reference: [site*D+mu][a], src/core/fields.hpp:46-57)
-//   phi [lat][k][site]           complex R     (reference: [site*d+k], src/core/scalar_field.hpp:15)
+//   P   [lat][mu][site/32][a][site%32]  real R     (reference: [site*D+mu][a], src/core/fields.hpp:46-57)
+//   phi [lat][site/32][k][site%32]      complex R  (reference: [site*d+k], src/core/scalar_field.hpp:15)
 // R = double (FP64 mode) or float (FP32-MD mode).  Several lattices of unequal
 // extents live back to back; every kernel walks a table of Work items (lattice,
 // direction, first site, count), one per block, so a single launch covers all
@@ -84,6 +84,18 @@ template <typename C, typename R> __device__ __forceinline__ void stc(R* p, long
 // Element index of component c of link (mu, s); component c + k sits k * ULANE further on.
 __device__ __forceinline__ long long u_index(const LatDev& L, int nn, int mu, int c, int s) {
   return L.u_off + (long long)mu * nn * L.Vp + ((long long)(s / ULANE) * nn + c) * ULANE + (s % ULANE);
+}
+// Momenta P: [mu][site/32][a][site%32] (ng components, direction planes of ng * Vp)
+__device__ __forceinline__ long long p_index(const LatDev& L, int ng, int mu, int g, int s) {
+  return L.p_off + (long long)mu * ng * L.Vp + ((long long)(s / ULANE) * ng + g) * ULANE + (s % ULANE);
+}
+// Scalar fields phi, pi: [site/32][k][site%32] (d components)
+__device__ __forceinline__ long long f_index(const LatDev& L, int d, int k, int s) {
+  return L.f_off + ((long long)(s / ULANE) * d + k) * ULANE + (s % ULANE);
+}
+// General-irrep scratch psi_f, psi_b: [mu][site/32][k][site%32]
+__device__ __forceinline__ long long g_index(const LatDev& L, int d, int mu, int k, int s) {
+  return L.g_off + (long long)mu * d * L.Vp + ((long long)(s / ULANE) * d + k) * ULANE + (s % ULANE);
 }
 template <int N, typename C, typename R>
 __device__ __forceinline__ Mat<N, C> ld_link(const R* __restrict__ U, const LatDev& L, int mu, int s) {
@@ -226,8 +238,8 @@ __device__ __forceinline__ void kick_link(const KickArgs& a, const LatDev& L, in
     cx<C> px[d], py[d];
 #pragma unroll
     for (int k = 0; k < d; ++k) {
-      px[k] = ldc<C>(phi, L.f_off + (long long)k * L.V + s);
-      py[k] = ldc<C>(phi, L.f_off + (long long)k * L.V + spm);
+      px[k] = ldc<C>(phi, f_index(L, d, k, s));
+      py[k] = ldc<C>(phi, f_index(L, d, k, spm));
     }
     const C kap = (C)L.kappa;
     if (REP == REP_FUND) {
@@ -253,15 +265,15 @@ __device__ __forceinline__ void kick_link(const KickArgs& a, const LatDev& L, in
   C F[N * N - 1];
   im_tr_proj<N, C>(Om, F);
   constexpr int ng = N * N - 1;
-  const long long pb = L.p_off + (long long)mu * ng * L.V + s;
+  const long long pb = p_index(L, ng, mu, 0, s);
   if (a.mode == M_UPDATE) {
     R* P = (R*)a.P;
     const C eps = (C)a.eps;
 #pragma unroll
-    for (int g = 0; g < ng; ++g) P[pb + (long long)g * L.V] = (R)((C)P[pb + (long long)g * L.V] - eps * F[g]);
+    for (int g = 0; g < ng; ++g) P[pb + g * ULANE] = (R)((C)P[pb + g * ULANE] - eps * F[g]);
   } else {
 #pragma unroll
-    for (int g = 0; g < ng; ++g) a.out[pb + (long long)g * L.V] = (double)F[g];
+    for (int g = 0; g < ng; ++g) a.out[pb + g * ULANE] = (double)F[g];
   }
 }
 
@@ -276,7 +288,7 @@ __device__ __forceinline__ void kick_site(const KickArgs& a, const LatDev& L, in
     cx<C> F[d], v[d], o[d];
     C n2 = C(0);
 #pragma unroll
-    for (int k = 0; k < d; ++k) { v[k] = ldc<C>(phi, L.f_off + (long long)k * L.V + s); n2 += norm2(v[k]); }
+    for (int k = 0; k < d; ++k) { v[k] = ldc<C>(phi, f_index(L, d, k, s)); n2 += norm2(v[k]); }
     const C cc = C(1) + C(2) * (C)L.lambda * (n2 - C(1));
 #pragma unroll
     for (int k = 0; k < d; ++k) F[k] = scale(v[k], C(-2) * cc);
@@ -285,13 +297,13 @@ __device__ __forceinline__ void kick_site(const KickArgs& a, const LatDev& L, in
       const int yf = nfwd(L, s, x[mu], mu), yb = nbwd(L, s, x[mu], mu);
       cx<C> o2[d];
 #pragma unroll
-      for (int k = 0; k < d; ++k) v[k] = ldc<C>(phi, L.f_off + (long long)k * L.V + yf);
+      for (int k = 0; k < d; ++k) v[k] = ldc<C>(phi, f_index(L, d, k, yf));
       {
         const Mat<N, C> Uf = ld_link<N, C>(U, L, mu, s);
         if (REP == REP_FUND) fund_apply<N, C>(Uf, v, o, false); else adj_apply<N, C>(Uf, v, o, false);
       }
 #pragma unroll
-      for (int k = 0; k < d; ++k) v[k] = ldc<C>(phi, L.f_off + (long long)k * L.V + yb);
+      for (int k = 0; k < d; ++k) v[k] = ldc<C>(phi, f_index(L, d, k, yb));
       {
         const Mat<N, C> Ub = ld_link<N, C>(U, L, mu, yb);
         if (REP == REP_FUND) fund_apply<N, C>(Ub, v, o2, true); else adj_apply<N, C>(Ub, v, o2, true);
@@ -299,35 +311,35 @@ __device__ __forceinline__ void kick_site(const KickArgs& a, const LatDev& L, in
 #pragma unroll
       for (int k = 0; k < d; ++k) F[k] = add(F[k], scale(add(o[k], o2[k]), kap2));
     }
-    const long long fb = L.f_off + s;
+    const long long fb = f_index(L, d, 0, s);
     if (a.mode == M_UPDATE) {
       R* pi = (R*)a.pi;
       const C eps = (C)a.eps;
 #pragma unroll
-      for (int k = 0; k < d; ++k) stc<C>(pi, fb + (long long)k * L.V, add(ldc_rw<C>(pi, fb + (long long)k * L.V), scale(F[k], eps)));
+      for (int k = 0; k < d; ++k) stc<C>(pi, fb + k * ULANE, add(ldc_rw<C>(pi, fb + k * ULANE), scale(F[k], eps)));
     } else {
       double2* out = reinterpret_cast<double2*>(a.out);
 #pragma unroll
-      for (int k = 0; k < d; ++k) out[fb + (long long)k * L.V] = make_double2((double)F[k].re, (double)F[k].im);
+      for (int k = 0; k < d; ++k) out[fb + k * ULANE] = make_double2((double)F[k].re, (double)F[k].im);
     }
   } else if (REP == REP_GEN) {
     const int d = a.d;
     const R* psif = (const R*)a.psif;
     const R* psib = (const R*)a.psib;
     C n2 = C(0);
-    for (int k = 0; k < d; ++k) n2 += norm2(ldc<C>(phi, L.f_off + (long long)k * L.V + s));
+    for (int k = 0; k < d; ++k) n2 += norm2(ldc<C>(phi, f_index(L, d, k, s)));
     const C cc = C(1) + C(2) * (C)L.lambda * (n2 - C(1));
     int yb[D];
 #pragma unroll
     for (int mu = 0; mu < D; ++mu) yb[mu] = nbwd(L, s, x[mu], mu);
     for (int k = 0; k < d; ++k) {
-      cx<C> F = scale(ldc<C>(phi, L.f_off + (long long)k * L.V + s), C(-2) * cc);
+      cx<C> F = scale(ldc<C>(phi, f_index(L, d, k, s)), C(-2) * cc);
 #pragma unroll
       for (int mu = 0; mu < D; ++mu) {
-        const long long gb = L.g_off + ((long long)mu * d + k) * L.V;
-        F = add(F, scale(add(ldc<C>(psif, gb + s), ldc<C>(psib, gb + yb[mu])), kap2));
+        
+        F = add(F, scale(add(ldc<C>(psif, g_index(L, d, mu, k, s)), ldc<C>(psib, g_index(L, d, mu, k, yb[mu]))), kap2));
       }
-      const long long fi = L.f_off + (long long)k * L.V + s;
+      const long long fi = f_index(L, d, k, s);
       if (a.mode == M_UPDATE) {
         R* pi = (R*)a.pi;
         stc<C>(pi, fi, add(ldc_rw<C>(pi, fi), scale(F, (C)a.eps)));
@@ -455,8 +467,8 @@ __global__ void __launch_bounds__(GEN_WARPS * 32) k_gen_links(const GenArgs a) {
   const int spm = nfwd(L, s, x[mu], mu);
   const Mat<N, C> M = ld_link<N, C>(U, L, mu, s);
   for (int k = lane; k < d; k += 32) {
-    px[k] = ldc<C>(phi, L.f_off + (long long)k * L.V + s);
-    py[k] = ldc<C>(phi, L.f_off + (long long)k * L.V + spm);
+    px[k] = ldc<C>(phi, f_index(L, d, k, s));
+    py[k] = ldc<C>(phi, f_index(L, d, k, spm));
   }
   __syncwarp();
   gen_apply<N, C>(a.t, M, false, py, buf, pf, lane);
@@ -464,7 +476,7 @@ __global__ void __launch_bounds__(GEN_WARPS * 32) k_gen_links(const GenArgs a) {
   R* psif = (R*)a.psif;
   R* psib = (R*)a.psib;
   for (int k = lane; k < d; k += 32) {
-    const long long gi = L.g_off + ((long long)mu * d + k) * L.V + s;
+    const long long gi = g_index(L, d, mu, k, s);
     stc<C>(psif, gi, pf[k]);
     if (a.mode != 1) stc<C>(psib, gi, pb[k]);
   }
@@ -483,7 +495,7 @@ __global__ void __launch_bounds__(GEN_WARPS * 32) k_gen_links(const GenArgs a) {
       z = cfma_cj(z, px[i], ti);
     }
     const C F = -(C)L.kappa * (C(-2) * z.im);
-    const long long pi_ = L.p_off + ((long long)mu * ng + g) * L.V + s;
+    const long long pi_ = p_index(L, ng, mu, g, s);
     if (a.mode == 0) {
       R* P = (R*)a.P;
       P[pi_] = (R)((C)P[pi_] - (C)a.eps * F);
@@ -560,9 +572,9 @@ __global__ void __launch_bounds__(KBLOCK) k_drift(const DriftArgs a) {
     constexpr int ng = N * N - 1;
     const R* P = (const R*)a.P;
     R v[ng];
-    const long long pb = L.p_off + (long long)mu * ng * L.V + s;
+    const long long pb = p_index(L, ng, mu, 0, s);
 #pragma unroll
-    for (int g = 0; g < ng; ++g) v[g] = P[pb + (long long)g * L.V];
+    for (int g = 0; g < ng; ++g) v[g] = P[pb + g * ULANE];
     Mat<N, R> H = alg_to_mat<N, R>(v);
 #pragma unroll
     for (int i = 0; i < N * N; ++i) H.e[i] = scale(H.e[i], (R)a.eps);
@@ -575,7 +587,7 @@ __global__ void __launch_bounds__(KBLOCK) k_drift(const DriftArgs a) {
     R* phi = (R*)a.phi;
     const R* pi = (const R*)a.pi;
     for (int k = 0; k < a.d; ++k) {
-      const long long i = L.f_off + (long long)k * L.V + s;
+      const long long i = f_index(L, a.d, k, s);
       stc<C>(phi, i, add(ldc_rw<C>(phi, i), scale(ldc<C>(pi, i), (C)a.eps)));
     }
   }
@@ -651,7 +663,7 @@ __global__ void __launch_bounds__(KBLOCK) k_measure(const MeasArgs a) {
     for (int mu = 0; mu < D; ++mu)
 #pragma unroll
       for (int g = 0; g < ng; ++g) {
-        const double p = (double)P[L.p_off + ((long long)mu * ng + g) * L.V + s];
+        const double p = (double)P[p_index(L, ng, mu, g, s)];
         r[3] += p * p;
       }
     if (a.scalar) {
@@ -659,8 +671,8 @@ __global__ void __launch_bounds__(KBLOCK) k_measure(const MeasArgs a) {
       const R* pi = (const R*)a.pi;
       double n2 = 0.0;
       for (int k = 0; k < a.d; ++k) {
-        n2 += norm2(ldc<double>(phi, L.f_off + (long long)k * L.V + s));
-        r[4] += norm2(ldc<double>(pi, L.f_off + (long long)k * L.V + s));
+        n2 += norm2(ldc<double>(phi, f_index(L, a.d, k, s)));
+        r[4] += norm2(ldc<double>(pi, f_index(L, a.d, k, s)));
       }
       r[5] = n2;
       r[1] = n2 + L.lambda * (n2 - 1.0) * (n2 - 1.0);
@@ -668,12 +680,12 @@ __global__ void __launch_bounds__(KBLOCK) k_measure(const MeasArgs a) {
         constexpr int d = RepDim<N, REP>::d;
         cx<double> px[d], py[d], o[d];
 #pragma unroll
-        for (int k = 0; k < d; ++k) px[k] = ldc<double>(phi, L.f_off + (long long)k * L.V + s);
+        for (int k = 0; k < d; ++k) px[k] = ldc<double>(phi, f_index(L, d, k, s));
 #pragma unroll
         for (int mu = 0; mu < D; ++mu) {
           const int y = nfwd(L, s, x[mu], mu);
 #pragma unroll
-          for (int k = 0; k < d; ++k) py[k] = ldc<double>(phi, L.f_off + (long long)k * L.V + y);
+          for (int k = 0; k < d; ++k) py[k] = ldc<double>(phi, f_index(L, d, k, y));
           const Mat<N, double> Umu = ld_link<N, double>(U, L, mu, s);
           if (REP == REP_FUND) fund_apply<N, double>(Umu, py, o, false); else adj_apply<N, double>(Umu, py, o, false);
           double h = 0.0;
@@ -687,8 +699,8 @@ __global__ void __launch_bounds__(KBLOCK) k_measure(const MeasArgs a) {
         for (int mu = 0; mu < D; ++mu) {
           double h = 0.0;
           for (int k = 0; k < a.d; ++k) {
-            const cx<double> p = ldc<double>(phi, L.f_off + (long long)k * L.V + s);
-            const cx<double> o = ldc<double>(psif, L.g_off + ((long long)mu * a.d + k) * L.V + s);
+            const cx<double> p = ldc<double>(phi, f_index(L, a.d, k, s));
+            const cx<double> o = ldc<double>(psif, g_index(L, a.d, mu, k, s));
             h += p.re * o.re + p.im * o.im;
           }
           r[2] += h;
@@ -808,7 +820,7 @@ __global__ void __launch_bounds__(KBLOCK) k_restore(const RestoreArgs a) {
     for (int c = 0; c < NN; ++c) reinterpret_cast<V*>(a.U)[b + c * ULANE] = reinterpret_cast<const V*>(a.Us)[b + c * ULANE];
   } else {
     for (int k = 0; k < a.d; ++k) {
-      const long long i = L.f_off + (long long)k * L.V + s;
+      const long long i = f_index(L, a.d, k, s);
       reinterpret_cast<V*>(a.phi)[i] = reinterpret_cast<const V*>(a.phis)[i];
     }
   }
@@ -867,9 +879,9 @@ __global__ void __launch_bounds__(KBLOCK) k_init(const InitArgs a) {
     } else if (a.what == 1 || a.what == 3) {
       const unsigned long long st = (a.what == 1) ? ghrng::key(a.pure ? 0xA1 : 0xC3, L.traj) : a.stream;
       R* P = (R*)a.P;
-      const long long pb = L.p_off + (long long)mu * ng * L.V + s;
+      const long long pb = p_index(L, ng, mu, 0, s);
 #pragma unroll
-      for (int g = 0; g < ng; ++g) P[pb + (long long)g * L.V] = (R)gauss_r<R>(L.seed, ghrng::key(st, s, mu, g));
+      for (int g = 0; g < ng; ++g) P[pb + g * ULANE] = (R)gauss_r<R>(L.seed, ghrng::key(st, s, mu, g));
     }
     return;
   }
@@ -882,11 +894,11 @@ __global__ void __launch_bounds__(KBLOCK) k_init(const InitArgs a) {
     for (int k = 0; k < a.d; ++k) {
       const double re = sg * gauss_r<R>(L.seed, ghrng::key(st, s, 2 * k));
       const double im = a.real ? 0.0 : sg * gauss_r<R>(L.seed, ghrng::key(st, s, 2 * k + 1));
-      stc<double>(vec, L.f_off + (long long)k * L.V + s, mk<double>(re, im));
+      stc<double>(vec, f_index(L, a.d, k, s), mk<double>(re, im));
     }
   } else if (a.what == 5) {
     R* vec = (R*)a.vec;
-    for (int k = 0; k < a.d; ++k) stc<double>(vec, L.f_off + (long long)k * L.V + s, mk<double>(k == 0 ? a.sigma : 0.0, 0.0));
+    for (int k = 0; k < a.d; ++k) stc<double>(vec, f_index(L, a.d, k, s), mk<double>(k == 0 ? a.sigma : 0.0, 0.0));
   }
 }
 
@@ -942,12 +954,12 @@ __global__ void k_xfer(const XferArgs a) {
     const int s = (int)(e / per_site);
     const int r = (int)(e % per_site);
     if (a.kind == 1) {
-      const long long di = L.p_off + (long long)r * L.V + s;   // r = mu*ng + g
+      const long long di = p_index(L, a.ncomp, r / a.ncomp, r % a.ncomp, s);   // r = mu*ng + g
       R* P = (R*)a.dev;
       if (a.to_dev) P[di] = (R)a.host_aos[e]; else a.host_aos[e] = (double)P[di];
     } else {
       // r = mu*NN + c (links) or k (vectors)
-      const long long di = (a.kind == 0) ? u_index(L, a.ncomp, r / a.ncomp, r % a.ncomp, s) : L.f_off + (long long)r * L.V + s;
+      const long long di = (a.kind == 0) ? u_index(L, a.ncomp, r / a.ncomp, r % a.ncomp, s) : f_index(L, a.ncomp, r, s);
       if (a.to_dev) stc<double>((R*)a.dev, di, mk<double>(a.host_aos[2 * e], a.host_aos[2 * e + 1]));
       else { const cx<double> z = ldc_rw<double>((const R*)a.dev, di); a.host_aos[2 * e] = z.re; a.host_aos[2 * e + 1] = z.im; }
     }
