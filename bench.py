@@ -268,7 +268,7 @@ def run_ours(a, dist):
         "data": "synthetic (reference counter-RNG hot start and Gaussian scalar field)",
         "config": {"workload": WORKLOAD, "lattice": WL["L"], "rep": "fundamental", "beta": WL["beta"],
                    "kappa": WL["kappa"], "lambda": WL["lam"], "integrator": "omelyan", "nmd": WL["nmd"],
-                   "tau": WL["tau"], "precision": "FP32 MD forces and links; FP64 H, exp(iH), reunitarisation",
+                   "tau": WL["tau"], "precision": "FP32 MD (fields, forces, exp(i eps P), SU(N) projection); FP64 H and Metropolis",
                    "l2": "flushed between trajectories (256 MB write, inside the timed region)",
                    "kick_tile": {"fp32": res["fp32"]["tile"], "fp64": res["fp64"]["tile"]},
                    "parallelism": f"replicas x{dist.world}"},
