@@ -7,6 +7,6 @@ the reference's C++ interface (GaugeHiggsHMC, GaugeHMC, the Representation
 classes), plus batched ensembles with on-device kappa tempering.
 """
 from ._lib import GaugeHiggsError, LIB_PATH  # noqa: F401  (raises ImportError if the library is missing)
-from .hmc import (AdjointRep, Ensemble, FundamentalRep, GaugeHiggsHMC, GaugeHMC, GeneralRep, LEAPFROG,  # noqa: F401
-                  OMELYAN, Representation, make_rep)
+from .hmc import (AdjointRep, CasimirChannels, Ensemble, FundamentalRep, GaugeHiggsHMC, GaugeHMC,  # noqa: F401
+                  GeneralRep, LEAPFROG, MultiInvariantPotential, OMELYAN, Representation, make_rep)
 

@@ -95,6 +95,10 @@ SIGNATURES = {
     "gh_temper_stats": [_ctx, _u64p, _u64p, _dp],
     "gh_rep_general_info": [C.c_int, _ip, C.c_int, _ip, _ip, C.POINTER(C.c_long)],
     "gh_rep_general_build": [C.c_int, _ip, C.c_int, _dp, _dp],
+    "gh_casimir_channels": [C.c_int, C.POINTER(RepDesc), _dp, C.c_int, _ip],
+    "gh_multi_superop": [C.c_int, C.POINTER(RepDesc), C.c_int, _dp, _dp],
+    "gh_set_potential_multi": [_ctx, C.c_int, _dp, C.c_double],
+    "gh_set_potential_quartic": [_ctx],
     "gh_plaquette_noalloc": [C.c_int, C.c_int, _ip, C.c_void_p, C.c_void_p, C.c_void_p],
     "gh_mlp_create": [C.c_int, _ip, C.c_int, C.c_uint64, C.POINTER(C.c_void_p)],
     "gh_mlp_destroy": [C.c_void_p],

@@ -11,6 +11,7 @@
 #include <string>
 #include <vector>
 #include "gh_engine.cuh"
+#include "gh_potential.h"
 #include "../../include/gauge_higgs_b200.h"
 
 using namespace ghk;
@@ -50,9 +51,17 @@ struct gh_ctx {
   // tiled kick work table (rebuilt when tile shapes change)
   Work* wk_dev = nullptr;
   size_t wk_cap = 0;
+  // general irreps: host copy of the generators T^a_R (multi-invariant potential set-up)
+  std::vector<double> T_host;
+  // multi-invariant potential: device copies of the channel superoperator
+  double2* asup64 = nullptr;
+  float2* asup32 = nullptr;
+  size_t asup_cap = 0;
   ~gh_ctx() {
     if (st) cudaStreamSynchronize(st);
     if (wk_dev) cudaFree(wk_dev);
+    if (asup64) cudaFree(asup64);
+    if (asup32) cudaFree(asup32);
     if (gexec) cudaGraphExecDestroy(gexec);
     if (graph) cudaGraphDestroy(graph);
     for (void* p : allocs) cudaFree(p);
@@ -344,6 +353,7 @@ int build_general(gh_ctx* ctx, const gh_rep_desc* r) {
   if (dimT > 200000) return fail(ctx, GH_ERR_REP, "N^n exceeds the 200000 cap of the reference (src/rep/rep_general.hpp:34)");
   const double* W = r->W;
   const double* T = r->T;
+  ctx->T_host.assign(T, T + 2 * (size_t)ng * d * d);
   std::vector<int> wt_ptr(dimT + 1, 0), wt_l, w_ptr(d + 1, 0), w_i, t_ptr(ng * d + 1, 0), t_j;
   std::vector<double2> wt_v, w_v, t_v;
   for (long i = 0; i < dimT; ++i) {
@@ -855,6 +865,51 @@ int gh_autotune(gh_ctx* ctx, int reps, double* best_ms) {
   cudaEventDestroy(e1);
   if (best_ms) *best_ms = total_best;
   return rebuild_kick_table(ctx);
+}
+
+// Multi-invariant onsite potential (src/action/scalar_invariants.hpp:190-206): the
+// channel superoperator is built on the host (gh_potential.cpp) and copied to the
+// device in both precisions; the kick's site items and the measure kernel apply it.
+int gh_set_potential_multi(gh_ctx* ctx, int n_channels, const double* f, double mu2) {
+  if (!ctx) return fail(nullptr, GH_ERR_ARG, "null context");
+  if (!ctx->scalar) return fail(ctx, GH_ERR_STATE, "no scalar field in a pure-gauge context");
+  if (n_channels < 0 || (n_channels > 0 && !f)) return fail(ctx, GH_ERR_ARG, "null couplings");
+  const int kind = ctx->rep == REP_FUND ? GH_REP_FUND : ctx->rep == REP_ADJ ? GH_REP_ADJ : GH_REP_GENERAL;
+  std::vector<double> c2, A;
+  std::string err;
+  int rc = ghpot::superop(ctx->N, kind, ctx->d, ctx->T_host.empty() ? nullptr : ctx->T_host.data(),
+                          std::vector<double>(f, f + n_channels), c2, A, err);
+  if (rc) return fail(ctx, rc, err);
+  const size_t n = (size_t)ctx->d * ctx->d * ctx->d * ctx->d;
+  CK(cudaStreamSynchronize(ctx->st));
+  if (n > ctx->asup_cap) {
+    if (ctx->asup64) cudaFree(ctx->asup64);
+    if (ctx->asup32) cudaFree(ctx->asup32);
+    ctx->asup64 = nullptr;
+    ctx->asup32 = nullptr;
+    ctx->asup_cap = 0;
+    CK(cudaMalloc(&ctx->asup64, n * sizeof(double2)));
+    CK(cudaMalloc(&ctx->asup32, n * sizeof(float2)));
+    ctx->asup_cap = n;
+  }
+  std::vector<float2> a32(n);
+  for (size_t i = 0; i < n; ++i) a32[i] = make_float2((float)A[2 * i], (float)A[2 * i + 1]);
+  CK(cudaMemcpy(ctx->asup64, A.data(), n * sizeof(double2), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(ctx->asup32, a32.data(), n * sizeof(float2), cudaMemcpyHostToDevice));
+  ctx->b.asup64 = ctx->asup64;
+  ctx->b.asup32 = ctx->asup32;
+  ctx->b.pot = POT_MULTI;
+  ctx->b.mu2 = mu2;
+  invalidate_graph(ctx);
+  return GH_OK;
+}
+
+int gh_set_potential_quartic(gh_ctx* ctx) {
+  if (!ctx) return fail(nullptr, GH_ERR_ARG, "null context");
+  CK(cudaStreamSynchronize(ctx->st));
+  ctx->b.pot = POT_QUARTIC;
+  invalidate_graph(ctx);
+  return GH_OK;
 }
 
 int gh_use_graph(gh_ctx* ctx, int enable) {

@@ -23,6 +23,10 @@ struct Bufs {
   int hist_cap;
   GenTables gen;
   int nlat, D, N, d, rep, scalar;
+  int pot;               // POT_QUARTIC or POT_MULTI
+  double mu2;
+  const double2* asup64; // multi-invariant potential superoperator, FP64 and FP32 copies
+  const float2* asup32;
   cudaStream_t st;
 };
 
@@ -57,6 +61,8 @@ struct Engine : EngineBase {
     KickArgs a;
     a.lats = b.lats; a.U = b.U; a.P = b.P; a.phi = b.phi; a.pi = b.pi; a.psif = b.psif; a.psib = b.psib;
     a.eps = eps; a.mode = mode; a.flags = flags; a.d = b.d; a.out = out;
+    a.pot = b.pot; a.mu2 = b.mu2;
+    a.asup = sizeof(R) == sizeof(double) ? (const void*)b.asup64 : (const void*)b.asup32;
     const bool do_sites = sites && b.scalar;
     const int first = links ? 0 : b.nwk_links;
     const int count = (links ? b.nwk_links : 0) + (do_sites ? b.nwk_sites : 0);
@@ -88,6 +94,7 @@ struct Engine : EngineBase {
     MeasArgs a;
     a.work = b.w_all + b.nw_links; a.lats = b.lats; a.U = b.U; a.P = b.P; a.phi = b.phi; a.pi = b.pi;
     a.psif = b.psif; a.d = b.d; a.scalar = b.scalar; a.partials = b.partials;
+    a.pot = b.pot; a.mu2 = b.mu2; a.asup = b.asup64;
     k_measure<D, N, R, REP><<<b.nw_sites, KBLOCK, 0, b.st>>>(a);
   }
   void init(const Bufs& b, InitArgs a, bool links, bool sites) override {

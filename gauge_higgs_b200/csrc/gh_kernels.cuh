@@ -35,6 +35,8 @@ constexpr int KICK_BLOCK = 1 << KICK_LOG2;
 constexpr int GEN_WARPS = 4;   // warps per block of the general-irrep kernel
 constexpr int NRED = 6;        // per-site partial sums of the measure kernel
 constexpr int ULANE = 32;      // sites per block of the link-field layout
+enum { POT_QUARTIC = 0, POT_MULTI = 1 };
+constexpr int POT_DMAX = 32;   // largest representation the multi-invariant potential accepts
 
 struct LatDev {
   int L[4];
@@ -201,6 +203,9 @@ struct KickArgs {
   int flags;          // F_GAUGE | F_MATTER
   int d;              // rep dimension (general irreps)
   double* out;        // M_WRITE destination (SoA like P / like phi, FP64)
+  int pot;            // POT_QUARTIC or POT_MULTI
+  double mu2;         // multi-invariant potential: -mu2 phi^dag phi
+  const void* asup;   // multi-invariant potential: A = sum_c 2 f_c P_c in the field precision
 };
 
 // The direction is a template parameter so that every index into the lattice
@@ -277,6 +282,46 @@ __device__ __forceinline__ void kick_link(const KickArgs& a, const LatDev& L, in
   }
 }
 
+// ---------------------------------------------------------------------------
+// Multi-invariant onsite potential at site s (src/action/scalar_invariants.hpp):
+// with M = phi phi^dag and A = sum_c 2 f_c P_c the combined channel superoperator
+// ((d^2) x (d^2), vec index i*d + j),
+//   w = A(M) phi,  dV/dphi^* = -mu2 phi + w,  V = -mu2 phi^dag phi + Re(phi^dag w) / 2.
+// Writes w (when given) and returns V.  One thread per site; d^4 complex
+// multiply-adds with A read through L1 (all threads of a warp read the same entry).
+// ---------------------------------------------------------------------------
+template <typename C, typename R>
+__device__ __noinline__ C pot_multi(const R* phi, const LatDev& L, int d, int s, const typename V2<C>::t* __restrict__ A,
+                                    C mu2, cx<C>* w) {
+  cx<C> p[POT_DMAX];
+  C n2 = C(0);
+  for (int k = 0; k < d; ++k) {
+    p[k] = ldc<C>(phi, f_index(L, d, k, s));
+    n2 += norm2(p[k]);
+  }
+  const int dd = d * d;
+  C re = C(0);
+  for (int r = 0; r < d; ++r) {
+    cx<C> acc = zero<C>();
+    for (int q = 0; q < d; ++q) {
+      const typename V2<C>::t* row = A + (size_t)(r * d + q) * dd;
+      cx<C> y = zero<C>();                 // A(M)_rq = sum_ij A_{rq,ij} phi_i conj(phi_j)
+      for (int i = 0; i < d; ++i) {
+        cx<C> t = zero<C>();
+        for (int j = 0; j < d; ++j) {
+          const typename V2<C>::t av = __ldg(row + i * d + j);
+          t = cfma_cj(t, p[j], mk<C>(av.x, av.y));
+        }
+        y = cfma(y, p[i], t);
+      }
+      acc = cfma(acc, y, p[q]);
+    }
+    if (w) w[r] = acc;
+    re = fmad(p[r].re, acc.re, fmad(p[r].im, acc.im, re));
+  }
+  return -mu2 * n2 + C(0.5) * re;
+}
+
 template <int D, int N, typename R, int REP>
 __device__ __forceinline__ void kick_site(const KickArgs& a, const LatDev& L, int s, const int* x) {
   typedef typename Cmp<R>::t C;
@@ -289,9 +334,16 @@ __device__ __forceinline__ void kick_site(const KickArgs& a, const LatDev& L, in
     C n2 = C(0);
 #pragma unroll
     for (int k = 0; k < d; ++k) { v[k] = ldc<C>(phi, f_index(L, d, k, s)); n2 += norm2(v[k]); }
-    const C cc = C(1) + C(2) * (C)L.lambda * (n2 - C(1));
+    if (a.pot == POT_MULTI) {          // -2 dV/dphi^* = 2 mu2 phi - 2 A(M) phi
+      cx<C> w[d];
+      pot_multi<C, R>(phi, L, d, s, (const typename V2<C>::t*)a.asup, (C)a.mu2, w);
 #pragma unroll
-    for (int k = 0; k < d; ++k) F[k] = scale(v[k], C(-2) * cc);
+      for (int k = 0; k < d; ++k) F[k] = sub(scale(v[k], C(2) * (C)a.mu2), scale(w[k], C(2)));
+    } else {                           // -2 dV/dphi^* = -2 [1 + 2 lambda (n2 - 1)] phi
+      const C cc = C(1) + C(2) * (C)L.lambda * (n2 - C(1));
+#pragma unroll
+      for (int k = 0; k < d; ++k) F[k] = scale(v[k], C(-2) * cc);
+    }
 #pragma unroll
     for (int mu = 0; mu < D; ++mu) {
       const int yf = nfwd(L, s, x[mu], mu), yb = nbwd(L, s, x[mu], mu);
@@ -329,11 +381,14 @@ __device__ __forceinline__ void kick_site(const KickArgs& a, const LatDev& L, in
     C n2 = C(0);
     for (int k = 0; k < d; ++k) n2 += norm2(ldc<C>(phi, f_index(L, d, k, s)));
     const C cc = C(1) + C(2) * (C)L.lambda * (n2 - C(1));
+    cx<C> w[POT_DMAX];
+    if (a.pot == POT_MULTI) pot_multi<C, R>(phi, L, d, s, (const typename V2<C>::t*)a.asup, (C)a.mu2, w);
     int yb[D];
 #pragma unroll
     for (int mu = 0; mu < D; ++mu) yb[mu] = nbwd(L, s, x[mu], mu);
     for (int k = 0; k < d; ++k) {
-      cx<C> F = scale(ldc<C>(phi, f_index(L, d, k, s)), C(-2) * cc);
+      const cx<C> pk = ldc<C>(phi, f_index(L, d, k, s));
+      cx<C> F = (a.pot == POT_MULTI) ? sub(scale(pk, C(2) * (C)a.mu2), scale(w[k], C(2))) : scale(pk, C(-2) * cc);
 #pragma unroll
       for (int mu = 0; mu < D; ++mu) {
         
@@ -633,6 +688,9 @@ struct MeasArgs {
   const void* phi;
   const void* pi;
   const void* psif;
+  int pot;
+  double mu2;
+  const double2* asup;   // multi-invariant potential superoperator (FP64)
   int d;
   int scalar;
   double* partials;   // [block][NRED]
@@ -685,7 +743,8 @@ __global__ void __launch_bounds__(KBLOCK) k_measure(const MeasArgs a) {
         r[4] += norm2(ldc<double>(pi, f_index(L, a.d, k, s)));
       }
       r[5] = n2;
-      r[1] = n2 + L.lambda * (n2 - 1.0) * (n2 - 1.0);
+      r[1] = (a.pot == POT_MULTI) ? pot_multi<double, R>(phi, L, a.d, s, a.asup, a.mu2, nullptr)
+                                  : n2 + L.lambda * (n2 - 1.0) * (n2 - 1.0);
       if (REP == REP_FUND || REP == REP_ADJ) {
         constexpr int d = RepDim<N, REP>::d;
         cx<double> px[d], py[d], o[d];

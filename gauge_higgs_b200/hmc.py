@@ -126,6 +126,59 @@ def make_rep(N, spec):
 
 
 # ---------------------------------------------------------------------------
+# Multi-invariant onsite potential (src/action/scalar_invariants.hpp)
+# ---------------------------------------------------------------------------
+class CasimirChannels:
+    """The quartic channels of R (x) Rbar: distinct eigenvalues C2 of the adjoint Casimir
+    superoperator sum_a [T^a_R, [T^a_R, .]], ascending (CasimirChannels<N>,
+    src/action/scalar_invariants.hpp:19-27).  Couplings f_c are given in this order."""
+
+    def __init__(self, rep):
+        self.rep = rep
+        c2 = np.zeros(rep.d * rep.d + 1)
+        n = C.c_int()
+        check(LIB.gh_casimir_channels(rep.N, C.byref(rep.desc()), _dptr(c2), len(c2), C.byref(n)))
+        self.c2 = c2[:n.value].copy()
+
+    @property
+    def lambda_(self):
+        return self.c2
+
+    def n_channels(self):
+        return len(self.c2)
+
+    def superop(self, f):
+        """A = sum_c 2 f_c P_c as a (d^2, d^2) complex matrix, vec index i*d + j."""
+        f = np.ascontiguousarray(f, np.float64)
+        d = self.rep.d
+        A = np.zeros((d * d, d * d), np.complex128)
+        check(LIB.gh_multi_superop(self.rep.N, C.byref(self.rep.desc()), len(f), _dptr(f), _dptr(A.view(np.float64))))
+        return A
+
+
+class MultiInvariantPotential:
+    """V = -mu2 phi^dag phi + sum_c f_c Tr(M^dag P_c M), M = phi phi^dag
+    (MultiInvariantPotential<N>, src/action/scalar_invariants.hpp:190-206).  Plug it in
+    with `hmc.potential = pot`; `hmc.potential = None` restores the quartic potential."""
+
+    def __init__(self, channels, f, mu2):
+        self.ch = channels
+        self.f = np.ascontiguousarray(f, np.float64)
+        self.mu2 = float(mu2)
+        if len(self.f) != channels.n_channels():
+            raise ValueError(f"need {channels.n_channels()} couplings, got {len(self.f)}")
+
+    def superop(self):
+        return self.ch.superop(self.f)
+
+    def value(self, phi):
+        """V of one d-vector (host evaluation through the same superoperator)."""
+        phi = np.asarray(phi, np.complex128)
+        w = (self.superop() @ np.outer(phi, phi.conj()).reshape(-1)).reshape(len(phi), len(phi)) @ phi
+        return -self.mu2 * float(np.vdot(phi, phi).real) + 0.5 * float(np.vdot(phi, w).real)
+
+
+# ---------------------------------------------------------------------------
 # Engine context
 # ---------------------------------------------------------------------------
 class _Context:
@@ -181,6 +234,21 @@ class Ensemble:
         lm = np.broadcast_to(np.asarray(lam, float), (self.n_lat,))
         for i in range(self.n_lat):
             self.ctx("gh_set_couplings", i, float(b[i]), float(k[i]), float(lm[i]))
+
+    # ---- onsite potential ----
+    @property
+    def potential(self):
+        return getattr(self, "_potential", None)
+
+    @potential.setter
+    def potential(self, pot):
+        """GaugeHiggsHMC::potential (src/hmc/gauge_higgs_hmc.hpp:25-27): a
+        MultiInvariantPotential for every lattice, or None for the quartic potential."""
+        if pot is None:
+            self.ctx("gh_set_potential_quartic")
+        else:
+            self.ctx("gh_set_potential_multi", len(pot.f), _dptr(pot.f), pot.mu2)
+        self._potential = pot
 
     # ---- couplings / integrator ----
     def set_couplings(self, lat, beta, kappa, lam):

@@ -267,6 +267,31 @@ double gh_rng_gauss(uint64_t seed, uint64_t key);
 int gh_rep_general_info(int N, const int* rows, int nrows, int* d, int* n_boxes, long* dimT);
 int gh_rep_general_build(int N, const int* rows, int nrows, double* T, double* W);
 
+/* ---- multi-invariant onsite potential ----
+ * V[phi] = -mu2 phi^dag phi + sum_c f_c Tr(M^dag P_c M), M = phi phi^dag, P_c the
+ * projector onto channel c of R (x) Rbar (an eigenspace of the adjoint Casimir
+ * superoperator sum_a [T^a_R, [T^a_R, .]]).  Replaces CasimirChannels<N>
+ * (src/action/scalar_invariants.hpp:19-27, channel search :152-187) and
+ * MultiInvariantPotential<N> plugged into GaugeHiggsHMC::potential
+ * (scalar_invariants.hpp:190-206, src/hmc/gauge_higgs_hmc.hpp:25-27).
+ * At most 32 components (d <= 32).
+ *
+ * gh_casimir_channels: the channels' Casimir values C2, ascending -- the order
+ *   in which couplings f_c are given (the reference's CasimirChannels::lambda).
+ *   rep->kind FUND / ADJ need only d; GENERAL needs rep->T.  Host only.
+ * gh_multi_superop: the combined superoperator A = sum_c 2 f_c P_c that the
+ *   device applies, [(p*d+q)*d*d + (i*d+j)] complex (re, im), as
+ *   MultiInvariantPotential::Asuper (scalar_invariants.hpp:100-118).  Host only.
+ * gh_set_potential_multi: every lattice of the context uses V from now on (the
+ *   quartic coupling lambda is ignored); n_channels must equal the number of
+ *   channels.  gh_set_potential_quartic returns to phi^dag phi + lambda
+ *   (phi^dag phi - 1)^2 (QuarticPotential, src/action/scalar_higgs.hpp:25-40), the
+ *   default.  Both invalidate a captured trajectory graph. */
+int gh_casimir_channels(int N, const gh_rep_desc* rep, double* c2, int cap, int* n_channels);
+int gh_multi_superop(int N, const gh_rep_desc* rep, int n_channels, const double* f, double* A);
+int gh_set_potential_multi(gh_ctx* ctx, int n_channels, const double* f, double mu2);
+int gh_set_potential_quartic(gh_ctx* ctx);
+
 #ifdef __cplusplus
 }
 #endif

@@ -538,15 +538,70 @@ static cx vdot(int d, const cx* x, const cx* y) {
 }
 
 /* scalar_higgs.hpp:43-65 with QuarticPotential::value :30-33 */
-double gho_scalar_action(const gho_lattice* lat, const gho_rep* r, const double* U,
-                         const double* phi, double kappa, double lambda) {
+/* Onsite potential: the quartic phi^dag phi + lambda (phi^dag phi - 1)^2
+ * (QuarticPotential, src/action/scalar_higgs.hpp:25-40) or the multi-invariant
+ * -mu2 phi^dag phi + sum_c f_c Tr(M^dag P_c M) given by its combined channel
+ * superoperator A = sum_c 2 f_c P_c (src/action/scalar_invariants.hpp:60-148):
+ * y = A vec(M), vec(M)[i*d+j] = phi_i conj(phi_j);  V = -mu2 n2 + Re <vec M, y> / 2;
+ * dV/dphibar = -mu2 phi + mat(y) phi. */
+typedef struct { int multi; double lambda; const double* A; double mu2; } gho_pot;
+
+static void multi_y(int d, const double* A, const cx* px, cx* y) {
+  const int dd = d * d;
+  for (int r = 0; r < dd; ++r) {
+    cx acc = cmk(0.0, 0.0);
+    for (int i = 0; i < d; ++i)
+      for (int j = 0; j < d; ++j) {
+        const cx a = cmk(A[2 * ((size_t)r * dd + i * d + j)], A[2 * ((size_t)r * dd + i * d + j) + 1]);
+        acc = cadd(acc, cmul(a, cmul(px[i], cconj(px[j]))));
+      }
+    y[r] = acc;
+  }
+}
+
+static double pot_value(const gho_pot* p, int d, const cx* px) {
+  const double n2 = vnorm2(d, px);
+  if (!p->multi) return n2 + p->lambda * (n2 - 1.0) * (n2 - 1.0);
+  cx* y = (cx*)malloc(sizeof(cx) * d * d);
+  multi_y(d, p->A, px, y);
+  double re = 0.0;
+  for (int i = 0; i < d; ++i)
+    for (int j = 0; j < d; ++j) re += cmul(cconj(cmul(px[i], cconj(px[j]))), y[i * d + j]).re;
+  free(y);
+  return -p->mu2 * n2 + 0.5 * re;
+}
+
+static void pot_dV(const gho_pot* p, int d, const cx* px, cx* g) {
+  if (!p->multi) {
+    const double c = 1.0 + 2.0 * p->lambda * (vnorm2(d, px) - 1.0);
+    for (int k = 0; k < d; ++k) g[k] = cmul(cmk(c, 0), px[k]);
+    return;
+  }
+  cx* y = (cx*)malloc(sizeof(cx) * d * d);
+  multi_y(d, p->A, px, y);
+  for (int k = 0; k < d; ++k) {
+    cx acc = cscal(px[k], -p->mu2);
+    for (int q = 0; q < d; ++q) acc = cadd(acc, cmul(y[k * d + q], px[q]));
+    g[k] = acc;
+  }
+  free(y);
+}
+
+void gho_multi_potential(int d, const double* A, double mu2, const double* phi, double* value, double* dV) {
+  const gho_pot p = {1, 0.0, A, mu2};
+  if (value) *value = pot_value(&p, d, (const cx*)phi);
+  if (dV) pot_dV(&p, d, (const cx*)phi, (cx*)dV);
+}
+
+/* scalar_higgs.hpp:43-65 */
+static double scalar_action_pot(const gho_lattice* lat, const gho_rep* r, const double* U,
+                                const double* phi, double kappa, const gho_pot* pot) {
   const int D = lat->D, N = lat->N, NN = N * N, d = r->d;
   cx* Dpy = (cx*)malloc(sizeof(cx) * d);
   double S = 0.0;
   for (int64_t s = 0; s < lat->vol; ++s) {
     const cx* px = (const cx*)phi + s * d;
-    const double n2 = vnorm2(d, px);
-    S += n2 + lambda * (n2 - 1.0) * (n2 - 1.0);
+    S += pot_value(pot, d, px);
     for (int mu = 0; mu < D; ++mu) {
       const cx* py = (const cx*)phi + gho_fwd(lat, s, mu) * d;
       gho_rep_rotate(r, (const double*)LINK(U, s, mu), (const double*)py, (double*)Dpy, 0);
@@ -554,21 +609,22 @@ double gho_scalar_action(const gho_lattice* lat, const gho_rep* r, const double*
     }
   }
   free(Dpy);
+  (void)NN;
   return S;
 }
 
-/* scalar_higgs.hpp:71-108 with QuarticPotential::dV_dphibar :34-39 */
-void gho_scalar_force(const gho_lattice* lat, const gho_rep* r, const double* U,
-                      const double* phi, double kappa, double lambda, double* Fphi) {
+/* scalar_higgs.hpp:71-108 */
+static void scalar_force_pot(const gho_lattice* lat, const gho_rep* r, const double* U,
+                             const double* phi, double kappa, const gho_pot* pot, double* Fphi) {
   const int D = lat->D, N = lat->N, NN = N * N, d = r->d;
   cx* Dpf = (cx*)malloc(sizeof(cx) * d);
   cx* Dpb = (cx*)malloc(sizeof(cx) * d);
   cx* F = (cx*)malloc(sizeof(cx) * d);
+  cx* g = (cx*)malloc(sizeof(cx) * d);
   for (int64_t s = 0; s < lat->vol; ++s) {
     const cx* px = (const cx*)phi + s * d;
-    const double n2 = vnorm2(d, px);
-    const double c = 1.0 + 2.0 * lambda * (n2 - 1.0);
-    for (int k = 0; k < d; ++k) { cx g = cmul(cmk(c, 0), px[k]); F[k] = cscal(g, -2.0); }
+    pot_dV(pot, d, px, g);
+    for (int k = 0; k < d; ++k) F[k] = cscal(g[k], -2.0);
     for (int mu = 0; mu < D; ++mu) {
       const int64_t yf = gho_fwd(lat, s, mu), yb = gho_bwd(lat, s, mu);
       gho_rep_rotate(r, (const double*)LINK(U, s, mu), (const double*)((const cx*)phi + yf * d), (double*)Dpf, 0);
@@ -577,7 +633,29 @@ void gho_scalar_force(const gho_lattice* lat, const gho_rep* r, const double* U,
     }
     memcpy((cx*)Fphi + s * d, F, sizeof(cx) * d);
   }
-  free(Dpf); free(Dpb); free(F);
+  free(Dpf); free(Dpb); free(F); free(g);
+  (void)NN;
+}
+
+double gho_scalar_action(const gho_lattice* lat, const gho_rep* r, const double* U,
+                         const double* phi, double kappa, double lambda) {
+  const gho_pot p = {0, lambda, NULL, 0.0};
+  return scalar_action_pot(lat, r, U, phi, kappa, &p);
+}
+void gho_scalar_force(const gho_lattice* lat, const gho_rep* r, const double* U,
+                      const double* phi, double kappa, double lambda, double* Fphi) {
+  const gho_pot p = {0, lambda, NULL, 0.0};
+  scalar_force_pot(lat, r, U, phi, kappa, &p, Fphi);
+}
+double gho_scalar_action_multi(const gho_lattice* lat, const gho_rep* r, const double* U,
+                               const double* phi, double kappa, const double* A, double mu2) {
+  const gho_pot p = {1, 0.0, A, mu2};
+  return scalar_action_pot(lat, r, U, phi, kappa, &p);
+}
+void gho_scalar_force_multi(const gho_lattice* lat, const gho_rep* r, const double* U,
+                            const double* phi, double kappa, const double* A, double mu2, double* Fphi) {
+  const gho_pot p = {1, 0.0, A, mu2};
+  scalar_force_pot(lat, r, U, phi, kappa, &p, Fphi);
 }
 
 /* scalar_higgs.hpp:113-128 */

@@ -92,6 +92,12 @@ void   gho_scalar_force(const gho_lattice* lat, const gho_rep* r, const double* 
 void   gho_add_matter_link_force(const gho_lattice* lat, const gho_rep* r, const double* U,
                                  const double* phi, double kappa, double* F);
 double gho_link_energy(const gho_lattice* lat, const gho_rep* r, const double* U, const double* phi);
+/* multi-invariant onsite potential from its channel superoperator A [(d^2) x (d^2)] complex */
+void   gho_multi_potential(int d, const double* A, double mu2, const double* phi, double* value, double* dV);
+double gho_scalar_action_multi(const gho_lattice* lat, const gho_rep* r, const double* U,
+                               const double* phi, double kappa, const double* A, double mu2);
+void   gho_scalar_force_multi(const gho_lattice* lat, const gho_rep* r, const double* U,
+                              const double* phi, double kappa, const double* A, double mu2, double* Fphi);
 double gho_higgs_length(const gho_lattice* lat, int d, const double* phi);
 double gho_polyakov(const gho_lattice* lat, const double* U, int tdir);
 double gho_kinetic_mom(const gho_lattice* lat, const double* P);

@@ -112,6 +112,10 @@ class Oracle:
         L.gho_scalar_force.argtypes = [C.c_void_p, C.c_void_p, _dp, _dp, C.c_double, C.c_double, _dp]
         L.gho_add_matter_link_force.argtypes = [C.c_void_p, C.c_void_p, _dp, _dp, C.c_double, _dp]
         L.gho_link_energy.restype = C.c_double
+        L.gho_scalar_action_multi.restype = C.c_double
+        L.gho_scalar_action_multi.argtypes = [C.c_void_p, C.c_void_p, _dp, _dp, C.c_double, _dp, C.c_double]
+        L.gho_scalar_force_multi.argtypes = [C.c_void_p, C.c_void_p, _dp, _dp, C.c_double, _dp, C.c_double, _dp]
+        L.gho_multi_potential.argtypes = [C.c_int, _dp, C.c_double, _dp, _dp, _dp]
         L.gho_link_energy.argtypes = [C.c_void_p, C.c_void_p, _dp, _dp]
         L.gho_higgs_length.restype = C.c_double
         L.gho_higgs_length.argtypes = [C.c_void_p, C.c_int, _dp]
@@ -233,6 +237,29 @@ class Oracle:
     def scalar_action(self, D, N, L, rep, U, phi, kappa, lam):
         lat = self.lattice(D, N, L)
         return self.lib.gho_scalar_action(C.byref(lat), C.byref(rep.s), _d(_cplx(U)), _d(_cplx(phi)), kappa, lam)
+
+    def multi_potential(self, d, A, mu2, phi):
+        A = np.ascontiguousarray(A, np.complex128)
+        phi = np.ascontiguousarray(phi, np.complex128)
+        g = np.zeros_like(phi)
+        v = C.c_double()
+        self.lib.gho_multi_potential(d, _d(A.view(np.float64)), mu2, _d(phi.view(np.float64)), C.byref(v),
+                                     _d(g.view(np.float64)))
+        return v.value, g
+
+    def scalar_force_multi(self, D, N, L, rep, U, phi, kappa, A, mu2):
+        lat = self.lattice(D, N, L)
+        A = np.ascontiguousarray(A, np.complex128)
+        Fp = np.zeros((lat.vol, rep.d), np.complex128)
+        self.lib.gho_scalar_force_multi(C.byref(lat), C.byref(rep.s), _d(_cplx(U)), _d(_cplx(phi)), kappa,
+                                        _d(A.view(np.float64)), mu2, _d(Fp.view(np.float64)))
+        return Fp
+
+    def scalar_action_multi(self, D, N, L, rep, U, phi, kappa, A, mu2):
+        lat = self.lattice(D, N, L)
+        A = np.ascontiguousarray(A, np.complex128)
+        return self.lib.gho_scalar_action_multi(C.byref(lat), C.byref(rep.s), _d(_cplx(U)), _d(_cplx(phi)), kappa,
+                                                _d(A.view(np.float64)), mu2)
 
     def link_energy(self, D, N, L, rep, U, phi):
         lat = self.lattice(D, N, L)
@@ -369,6 +396,14 @@ class Reference:
         L.ref_scalar_force.argtypes = [C.c_int, C.c_int, _ip, C.c_char_p, _dp, _dp, C.c_double, C.c_double, _dp]
         L.ref_scalar_action.restype = C.c_double
         L.ref_scalar_action.argtypes = [C.c_int, C.c_int, _ip, C.c_char_p, _dp, _dp, C.c_double, C.c_double]
+        L.ref_casimir_channels.argtypes = [C.c_int, C.c_char_p, _dp, C.c_int]
+        L.ref_multi_superop.argtypes = [C.c_int, C.c_char_p, _dp, C.c_int, C.c_double, _dp]
+        L.ref_multi_value_dV.argtypes = [C.c_int, C.c_char_p, _dp, C.c_int, C.c_double, _dp, _dp, _dp]
+        L.ref_scalar_force_multi.argtypes = [C.c_int, C.c_int, _ip, C.c_char_p, _dp, _dp, C.c_double, _dp, C.c_int,
+                                             C.c_double, _dp]
+        L.ref_scalar_action_multi.restype = C.c_double
+        L.ref_scalar_action_multi.argtypes = [C.c_int, C.c_int, _ip, C.c_char_p, _dp, _dp, C.c_double, _dp, C.c_int,
+                                              C.c_double]
         L.ref_link_energy.restype = C.c_double
         L.ref_link_energy.argtypes = [C.c_int, C.c_int, _ip, C.c_char_p, _dp, _dp]
         L.ref_hmc_op.argtypes = [C.c_int, C.c_int, C.c_int, _ip, C.c_char_p, _u64, C.c_double, C.c_double,
@@ -512,6 +547,49 @@ class Reference:
 
     def scalar_action(self, D, N, L, spec, U, phi, kappa, lam):
         return self.lib.ref_scalar_action(D, N, self._L(L), spec.encode(), _d(_cplx(U)), _d(_cplx(phi)), kappa, lam)
+
+    # multi-invariant onsite potential (src/action/scalar_invariants.hpp)
+    def casimir_channels(self, N, spec):
+        c2 = np.zeros(256)
+        n = self.lib.ref_casimir_channels(N, spec.encode(), _d(c2), len(c2))
+        if n < 0:
+            raise RuntimeError(f"ref_casimir_channels rc={n}")
+        return c2[:n].copy()
+
+    def multi_superop(self, N, spec, f, mu2):
+        d = self.rep_info(N, spec)["d"] if spec not in ("fund", "adj") else (N if spec == "fund" else N * N - 1)
+        f = np.ascontiguousarray(f, np.float64)
+        A = np.zeros((d * d, d * d), np.complex128)
+        rc = self.lib.ref_multi_superop(N, spec.encode(), _d(f), len(f), mu2, _d(A.view(np.float64)))
+        if rc:
+            raise RuntimeError(f"ref_multi_superop rc={rc}")
+        return A
+
+    def multi_value_dV(self, N, spec, f, mu2, phi):
+        f = np.ascontiguousarray(f, np.float64)
+        phi = np.ascontiguousarray(phi, np.complex128)
+        g = np.zeros_like(phi)
+        v = C.c_double()
+        rc = self.lib.ref_multi_value_dV(N, spec.encode(), _d(f), len(f), mu2, _d(phi.view(np.float64)), C.byref(v),
+                                         _d(g.view(np.float64)))
+        if rc:
+            raise RuntimeError(f"ref_multi_value_dV rc={rc}")
+        return v.value, g
+
+    def scalar_force_multi(self, D, N, L, spec, U, phi, kappa, f, mu2):
+        phi = np.ascontiguousarray(phi, np.complex128)
+        f = np.ascontiguousarray(f, np.float64)
+        Fp = np.zeros_like(phi)
+        rc = self.lib.ref_scalar_force_multi(D, N, self._L(L), spec.encode(), _d(_cplx(U)), _d(_cplx(phi)), kappa,
+                                             _d(f), len(f), mu2, _d(Fp.view(np.float64)))
+        if rc:
+            raise RuntimeError(f"ref_scalar_force_multi rc={rc}")
+        return Fp
+
+    def scalar_action_multi(self, D, N, L, spec, U, phi, kappa, f, mu2):
+        f = np.ascontiguousarray(f, np.float64)
+        return self.lib.ref_scalar_action_multi(D, N, self._L(L), spec.encode(), _d(_cplx(U)), _d(_cplx(phi)), kappa,
+                                                _d(f), len(f), mu2)
 
     def link_energy(self, D, N, L, spec, U, phi):
         return self.lib.ref_link_energy(D, N, self._L(L), spec.encode(), _d(_cplx(U)), _d(_cplx(phi)))

@@ -14,6 +14,7 @@
 #include "rep/rep_fundamental.hpp"
 #include "rep/rep_adjoint.hpp"
 #include "rep/rep_general.hpp"
+#include "action/scalar_invariants.hpp"
 #include <cstdint>
 #include <cstring>
 #include <map>
@@ -217,6 +218,53 @@ double ref_scalar_action(int D, int N, const int* L, const char* spec, const dou
 double ref_link_energy(int D, int N, const int* L, const char* spec, const double* U, const double* phi) {
 #define CALL(DD, NN) { auto* r = get_rep<NN>(spec); if (!r) return 0.0 / 0.0; Lattice<DD> lat(ext<DD>(L)); GaugeField<DD, NN> G(lat); load_U(G, U); \
     CVecField<DD> f(lat, r->d); load_V(f, phi); return link_energy<DD, NN>(f, G, *r); }
+  DISPATCH_DN(D, N, CALL)
+#undef CALL
+}
+
+// ---- multi-invariant onsite potential (src/action/scalar_invariants.hpp) ----
+// Channels: the distinct adjoint-Casimir eigenvalues of R (x) Rbar, in the
+// reference's order; returns their number (-1: bad N / spec).
+int ref_casimir_channels(int N, const char* spec, double* c2, int cap) {
+#define CALL(NN) { auto* r = get_rep<NN>(spec); if (!r) return -2; CasimirChannels<NN> ch(*r); \
+    const int n = ch.n_channels(); for (int c = 0; c < n && c < cap; ++c) c2[c] = ch.lambda[c]; return n; }
+  DISPATCH_N(N, CALL)
+#undef CALL
+}
+// The combined superoperator sum_c 2 f_c P_c as built by MultiInvariantPotential:
+// A[(p*d+q)*d*d + (i*d+j)] complex.
+int ref_multi_superop(int N, const char* spec, const double* f, int nf, double mu2, double* A) {
+#define CALL(NN) { auto* r = get_rep<NN>(spec); if (!r) return -2; CasimirChannels<NN> ch(*r); \
+    if (nf != ch.n_channels()) return -3; MultiInvariantPotential<NN> pot(ch, std::vector<Real>(f, f + nf), mu2); \
+    for (std::size_t k = 0; k < pot.Asuper.size(); ++k) { A[2 * k] = pot.Asuper[k].real(); A[2 * k + 1] = pot.Asuper[k].imag(); } \
+    return 0; }
+  DISPATCH_N(N, CALL)
+#undef CALL
+}
+// V(phi) and dV/dphibar of one d-vector.
+int ref_multi_value_dV(int N, const char* spec, const double* f, int nf, double mu2, const double* phi, double* value, double* g) {
+#define CALL(NN) { auto* r = get_rep<NN>(spec); if (!r) return -2; CasimirChannels<NN> ch(*r); \
+    if (nf != ch.n_channels()) return -3; MultiInvariantPotential<NN> pot(ch, std::vector<Real>(f, f + nf), mu2); \
+    const DVec v = load_dvec(r->d, phi); *value = pot.value(v); store_dvec(pot.dV_dphibar(v), g); return 0; }
+  DISPATCH_N(N, CALL)
+#undef CALL
+}
+int ref_scalar_force_multi(int D, int N, const int* L, const char* spec, const double* U, const double* phi, double kappa,
+                           const double* f, int nf, double mu2, double* Fphi) {
+#define CALL(DD, NN) { auto* r = get_rep<NN>(spec); if (!r) return -2; CasimirChannels<NN> ch(*r); \
+    if (nf != ch.n_channels()) return -3; MultiInvariantPotential<NN> pot(ch, std::vector<Real>(f, f + nf), mu2); \
+    Lattice<DD> lat(ext<DD>(L)); GaugeField<DD, NN> G(lat); load_U(G, U); \
+    CVecField<DD> fl(lat, r->d); load_V(fl, phi); CVecField<DD> Fp(lat, r->d); \
+    scalar_force<DD, NN>(fl, G, *r, kappa, pot, Fp); store_V(Fp, Fphi); return 0; }
+  DISPATCH_DN(D, N, CALL)
+#undef CALL
+}
+double ref_scalar_action_multi(int D, int N, const int* L, const char* spec, const double* U, const double* phi, double kappa,
+                               const double* f, int nf, double mu2) {
+#define CALL(DD, NN) { auto* r = get_rep<NN>(spec); if (!r) return 0.0 / 0.0; CasimirChannels<NN> ch(*r); \
+    if (nf != ch.n_channels()) return 0.0 / 0.0; MultiInvariantPotential<NN> pot(ch, std::vector<Real>(f, f + nf), mu2); \
+    Lattice<DD> lat(ext<DD>(L)); GaugeField<DD, NN> G(lat); load_U(G, U); \
+    CVecField<DD> fl(lat, r->d); load_V(fl, phi); return scalar_action<DD, NN>(fl, G, *r, kappa, pot); }
   DISPATCH_DN(D, N, CALL)
 #undef CALL
 }

@@ -128,7 +128,47 @@ def field_fixture(name, D, N, L, spec, beta, kappa, lam, nmd, integ, seed=1, eps
     np.savez_compressed(os.path.join(HERE, name + ".npz"), **out)
 
 
-if __name__ == "__main__":
+def multi_fixture():
+    """Multi-invariant onsite potential (src/action/scalar_invariants.hpp): channels,
+    the combined superoperator, V and dV/dphibar of single vectors, and the scalar
+    force and action of small lattices with that potential."""
+    out = {}
+    cases = [(2, "fund"), (2, "adj"), (3, "fund"), (3, "adj"), (2, "6"), (3, "2"), (3, "2,1:real")]
+    rng = np.random.default_rng(2026)
+    for N, spec in cases:
+        tag = f"N{N}_{spec.replace(',', '-').replace(':', '_')}"
+        c2 = R.casimir_channels(N, spec)
+        f = np.round(rng.uniform(0.2, 1.5, size=len(c2)), 3)
+        mu2 = 0.7
+        A = R.multi_superop(N, spec, f, mu2)
+        d = int(round(np.sqrt(A.shape[0])))
+        phis = rng.normal(size=(4, d)) + 1j * rng.normal(size=(4, d))
+        vals, dvs = [], []
+        for ph in phis:
+            v, g = R.multi_value_dV(N, spec, f, mu2, ph)
+            vals.append(v)
+            dvs.append(g)
+        out.update({tag + "_c2": c2, tag + "_f": f, tag + "_mu2": np.array(mu2), tag + "_A": A,
+                    tag + "_phi": phis, tag + "_value": np.array(vals), tag + "_dV": np.array(dvs)})
+    # lattices: scalar force and action with the potential
+    for name, D, N, L, spec in [("lat_su2_fund", 3, 2, [3, 4, 2], "fund"), ("lat_su3_adj", 3, 3, [2, 3, 2], "adj"),
+                                ("lat_su2_spin3", 2, 2, [3, 2], "6")]:
+        c2 = R.casimir_channels(N, spec)
+        f = np.round(rng.uniform(0.2, 1.5, size=len(c2)), 3)
+        U = R.hot_start(D, N, L, 5, 0.8)
+        d = R.multi_superop(N, spec, f, 0.0).shape[0]
+        d = int(round(np.sqrt(d)))
+        phi = R.phi_gaussian(D, L, d, 5, 12345, False, 0.6)
+        out.update({name + "_f": f, name + "_U": U, name + "_phi": phi, name + "_L": np.array(L),
+                    name + "_Fphi": R.scalar_force_multi(D, N, L, spec, U, phi, 0.17, f, 0.4),
+                    name + "_SH": np.array(R.scalar_action_multi(D, N, L, spec, U, phi, 0.17, f, 0.4))})
+    np.savez_compressed(os.path.join(HERE, "multi_potential.npz"), **out)
+
+
+if __name__ == "__main__" and sys.argv[1:] == ["multi"]:
+    multi_fixture()
+elif __name__ == "__main__":
+    multi_fixture()
     rng_fixture()
     rep_fixture()
     field_fixture("su3_fund_d4", 4, 3, [4, 3, 2, 3], "fund", 5.7, 0.10, 0.5, 4, OMELYAN)
