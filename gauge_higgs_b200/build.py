@@ -99,7 +99,8 @@ def build(force=False, jobs=None, verbose=False):
     return LIB
 
 
-DRIVERS = [("hmc_higgs", 4, 2), ("hmc_higgs_su3", 4, 3), ("gh_hmc", 4, 2), ("gh_hmc_su3", 4, 3)]
+DRIVERS = [("hmc_higgs", 4, 2), ("hmc_higgs_su3", 4, 3), ("gh_hmc", 4, 2), ("gh_hmc_su3", 4, 3),
+           ("hmc_higgs_multi", 4, 2), ("hmc_higgs_multi_su3", 4, 3)]
 
 
 def build_drivers(force=False):

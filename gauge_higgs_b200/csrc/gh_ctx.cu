@@ -411,6 +411,10 @@ extern "C" {
 
 const char* gh_last_error(const gh_ctx* ctx) { return ctx ? ctx->err.c_str() : g_err.c_str(); }
 
+namespace ghpot {
+void set_host_error(const std::string& m) { g_err = m; }
+}
+
 uint64_t gh_rng_key(uint64_t a, uint64_t b, uint64_t c, uint64_t d, uint64_t e) { return ghrng::key(a, b, c, d, e); }
 double gh_rng_uniform(uint64_t seed, uint64_t key) { return ghrng::uniform(seed, key); }
 double gh_rng_gauss(uint64_t seed, uint64_t key) { return ghrng::gauss(seed, key); }

@@ -287,11 +287,11 @@ int superop(int N, int kind, int d, const double* Tgen, const std::vector<double
 }  // namespace ghpot
 
 extern "C" int gh_casimir_channels(int N, const gh_rep_desc* rep, double* c2, int cap, int* n_channels) {
-  if (!rep) return GH_ERR_ARG;
+  if (!rep) { ghpot::set_host_error("null representation"); return GH_ERR_ARG; }
   std::vector<double> v;
   std::string err;
   const int rc = ghpot::channels(N, rep->kind, rep->d, rep->T, v, err);
-  if (rc) return rc;
+  if (rc) { ghpot::set_host_error(err); return rc; }
   if (n_channels) *n_channels = (int)v.size();
   if (c2)
     for (int c = 0; c < (int)v.size() && c < cap; ++c) c2[c] = v[c];
@@ -299,11 +299,11 @@ extern "C" int gh_casimir_channels(int N, const gh_rep_desc* rep, double* c2, in
 }
 
 extern "C" int gh_multi_superop(int N, const gh_rep_desc* rep, int n_channels, const double* f, double* A) {
-  if (!rep || !A || (n_channels > 0 && !f)) return GH_ERR_ARG;
+  if (!rep || !A || (n_channels > 0 && !f)) { ghpot::set_host_error("null representation, couplings or output"); return GH_ERR_ARG; }
   std::vector<double> c2, Av;
   std::string err;
   const int rc = ghpot::superop(N, rep->kind, rep->d, rep->T, std::vector<double>(f, f + std::max(n_channels, 0)), c2, Av, err);
-  if (rc) return rc;
+  if (rc) { ghpot::set_host_error(err); return rc; }
   std::copy(Av.begin(), Av.end(), A);
   return GH_OK;
 }

@@ -10,4 +10,6 @@ int channels(int N, int kind, int d, const double* Tgen, std::vector<double>& c2
 // The channels and A = sum_c 2 f_c P_c, [(p*d+q)*d*d + (i*d+j)] complex as re, im pairs.
 int superop(int N, int kind, int d, const double* Tgen, const std::vector<double>& f, std::vector<double>& c2,
             std::vector<double>& A, std::string& err);
+// Message of a failed context-free call, read back by gh_last_error(NULL) (gh_ctx.cu).
+void set_host_error(const std::string& m);
 }  // namespace ghpot

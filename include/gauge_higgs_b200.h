@@ -282,6 +282,7 @@ int gh_rep_general_build(int N, const int* rows, int nrows, double* T, double* W
  * gh_multi_superop: the combined superoperator A = sum_c 2 f_c P_c that the
  *   device applies, [(p*d+q)*d*d + (i*d+j)] complex (re, im), as
  *   MultiInvariantPotential::Asuper (scalar_invariants.hpp:100-118).  Host only.
+ *   The two host-only calls report errors through gh_last_error(NULL).
  * gh_set_potential_multi: every lattice of the context uses V from now on (the
  *   quartic coupling lambda is ignored); n_channels must equal the number of
  *   channels.  gh_set_potential_quartic returns to phi^dag phi + lambda

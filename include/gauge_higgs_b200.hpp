@@ -12,6 +12,7 @@
 //   GaugeHMC<D,N>            src/hmc/hmc.hpp:12-96 (pure gauge)
 //   observables              avg_plaquette, higgs_length, link_energy, polyakov_loop
 //   Stats                    src/measure/observables.hpp:104-145
+//   CasimirChannels, MultiInvariantPotential   src/action/scalar_invariants.hpp:19-206
 // Fields live on the GPU; U()/phi() copy them to host vectors in the reference's
 // layouts.  Errors throw std::runtime_error, as the reference does.
 #pragma once
@@ -86,6 +87,33 @@ template <int N> Representation make_rep(std::string spec) {
   return GeneralRep<N>(rows, real);
 }
 
+// ---- multi-invariant onsite potential (src/action/scalar_invariants.hpp) ----
+// CasimirChannels<N>(rep): the quartic channels of R (x) Rbar, lambda = their
+// adjoint-Casimir values, ascending (scalar_invariants.hpp:19-27).
+template <int N> struct CasimirChannels {
+  Representation rep;
+  std::vector<double> lambda;
+  explicit CasimirChannels(const Representation& R) : rep(R) {
+    const gh_rep_desc d = rep.desc();
+    int n = 0;
+    check(gh_casimir_channels(N, &d, nullptr, 0, &n), nullptr);
+    lambda.assign((size_t)n, 0.0);
+    check(gh_casimir_channels(N, &d, lambda.data(), n, &n), nullptr);
+  }
+  int n_channels() const { return (int)lambda.size(); }
+};
+// MultiInvariantPotential<N>(channels, f, mu2): V = -mu2 phi^dag phi + sum_c f_c V_c
+// (scalar_invariants.hpp:190-206); plug it in with hmc.potential = &pot.
+template <int N> struct MultiInvariantPotential {
+  const CasimirChannels<N>* ch = nullptr;
+  std::vector<double> f;
+  double mu2 = 0.0;
+  MultiInvariantPotential(const CasimirChannels<N>& c, std::vector<double> ff, double m) : ch(&c), f(std::move(ff)), mu2(m) {
+    if ((int)f.size() != c.n_channels())
+      throw std::runtime_error("need " + std::to_string(c.n_channels()) + " couplings, got " + std::to_string(f.size()));
+  }
+};
+
 // ---- HMC ----
 template <int D, int N>
 class GaugeHiggsHMC {
@@ -97,6 +125,8 @@ class GaugeHiggsHMC {
   std::uint64_t traj_count = 0, accept_count = 0;
   double last_dH = 0.0;
   int64_t vol = 1;
+  // optional onsite potential (src/hmc/gauge_higgs_hmc.hpp:25-27); nullptr = quartic in lambda
+  const MultiInvariantPotential<N>* potential = nullptr;
 
   GaugeHiggsHMC(const std::array<int, D>& extents, const Representation& R, std::uint64_t seed,
                 Precision prec = Precision::FP64)
@@ -192,6 +222,11 @@ class GaugeHiggsHMC {
       check(gh_set_traj_count(ctx_, 0, traj_count, accept_count), ctx_);
       ptc_ = traj_count; pac_ = accept_count;
     }
+    if (potential != ppot_) {
+      if (potential) check(gh_set_potential_multi(ctx_, (int)potential->f.size(), potential->f.data(), potential->mu2), ctx_);
+      else check(gh_set_potential_quartic(ctx_), ctx_);
+      ppot_ = potential;
+    }
   }
   void pull_counters() {
     std::uint64_t t, a, nf;
@@ -205,6 +240,7 @@ class GaugeHiggsHMC {
   double pb_ = NAN, pk_ = NAN, pl_ = NAN, pt_ = NAN;
   int pn_ = -1, pi_ = -1;
   std::uint64_t ptc_ = 0, pac_ = 0;
+  const MultiInvariantPotential<N>* ppot_ = nullptr;
 };
 
 template <int D, int N>
@@ -255,5 +291,55 @@ struct Stats {
     return std::sqrt(v / bm.size());
   }
 };
+
+// ---- autocorrelation analysis (src/measure/autocorr.hpp) ----
+// Madras-Sokal: autocovariance with 1/N normalisation, tau_int = 1/2 + sum_{t=1}^{W}
+// rho(t) with the smallest window W >= 6 tau_int(W) (lags capped at 2000 and N-1);
+// the error on the mean is sqrt(2 tau_int var / N).  A series with no fluctuations
+// (variance <= 1e-24 <x^2>) has tau_int = 1/2 and error 0.
+inline std::vector<double> autocovariance(const std::vector<double>& x, int maxlag) {
+  const int n = (int)x.size();
+  if (n == 0) return {};
+  double m = 0.0;
+  for (double v : x) m += v;
+  m /= n;
+  maxlag = std::min(maxlag < 0 ? n - 1 : maxlag, n - 1);
+  std::vector<double> c((size_t)maxlag + 1, 0.0);
+  for (int t = 0; t <= maxlag; ++t) {
+    double s = 0.0;
+    for (int i = 0; i + t < n; ++i) s += (x[i] - m) * (x[i + t] - m);
+    c[t] = s / n;
+  }
+  return c;
+}
+inline bool no_fluctuations(const std::vector<double>& x, double c0) {
+  double m2 = 0.0;
+  for (double v : x) m2 += v * v;
+  return c0 <= 1e-24 * (x.empty() ? 0.0 : m2 / x.size()) + 1e-300;
+}
+inline double tau_int(const std::vector<double>& x, int* window = nullptr) {
+  const int n = (int)x.size();
+  if (window) *window = 0;
+  if (n < 2) return 0.5;
+  const std::vector<double> c = autocovariance(x, std::min(n - 1, 2000));
+  if (no_fluctuations(x, c[0])) return 0.5;
+  double tau = 0.5;
+  int W = (int)c.size() - 1;
+  for (int M = 1; M < (int)c.size(); ++M) {
+    tau += c[M] / c[0];
+    if (M >= 6.0 * tau) { W = M; break; }
+  }
+  if (window) *window = W;
+  return std::max(tau, 0.5);
+}
+inline double effective_sample_size(const std::vector<double>& x) {
+  return x.empty() ? 0.0 : (double)x.size() / (2.0 * tau_int(x));
+}
+inline double autocorr_error(const std::vector<double>& x) {
+  if (x.size() < 2) return 0.0;
+  const double var = autocovariance(x, 0)[0];
+  if (no_fluctuations(x, var)) return 0.0;
+  return std::sqrt(2.0 * tau_int(x) * var / (double)x.size());
+}
 
 }  // namespace ghb

@@ -58,3 +58,25 @@ def test_driver_rejects_bad_rep():
     r = subprocess.run([os.path.join(BIN, "hmc_higgs_su3"), "1,2", "4", "5.7", "0.1", "0.5"], capture_output=True,
                        text=True, timeout=60)
     assert r.returncode == 1 and "rep error" in r.stderr
+
+
+def test_hmc_higgs_multi_runs():
+    """The multi-invariant potential driver (src/hmc_higgs_multi.cpp): channel listing,
+    a short run with explicit couplings, its output lines and the time-series file."""
+    exe = os.path.join(BIN, "hmc_higgs_multi")
+    r = subprocess.run([exe, "fund"], capture_output=True, text=True, timeout=60)
+    assert r.returncode == 0 and "2 quartic channels" in r.stdout
+    ts = os.path.join(ROOT, "gpurun_out", "multi_ts.txt") if os.path.isdir(os.path.join(ROOT, "gpurun_out")) else \
+        os.path.join("/tmp", "multi_ts.txt")
+    r = subprocess.run([exe, "fund", "4", "2.3", "0.2", "1.0", "0.8,0.5", "20", "60", "16", "1.0", "3", ts],
+                       capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr
+    v = parse(r.stdout)
+    assert 0.4 < v["plaquette"][0] < 0.8
+    assert v["acceptance"][0] > 0.6
+    assert "tau_int(L_link)" in r.stdout
+    with open(ts) as f:
+        assert len([ln for ln in f if not ln.startswith("#")]) == 60
+    r = subprocess.run([exe, "fund", "4", "2.3", "0.2", "1.0", "1,2,3"], capture_output=True, text=True, timeout=60)
+    assert r.returncode == 1 and "need 2 couplings" in r.stderr
+

@@ -114,3 +114,25 @@ def test_hmc_exp_minus_dH(precision):
     assert abs(mean - 1.0) < 0.12, (mean, acc)
     assert acc > 0.5, acc
     h.close()
+
+
+def test_unit_couplings_reproduce_quartic_hmc():
+    """f_c = 1, mu2 = 1 gives V = (phi^dag phi)^2 - phi^dag phi, the quartic potential at
+    lambda = 1 up to a constant: the same seeds give the same trajectories (to roundoff)."""
+    import gauge_higgs_b200 as gh
+    out = []
+    for multi in (False, True):
+        rep = gh.FundamentalRep(2)
+        h = gh.GaugeHiggsHMC([4, 4, 4, 4], rep, seed=23, beta=2.3, kappa=0.2, lam=1.0, nmd=12)
+        if multi:
+            ch = gh.CasimirChannels(rep)
+            h.potential = gh.MultiInvariantPotential(ch, np.ones(ch.n_channels()), 1.0)
+        h.hot(0.5)
+        h.phi_gaussian(12345, 0.5)
+        out.append(h.run(5)[:, 0])
+        h.close()
+    a, b = out
+    assert np.array_equal(a["accepted"], b["accepted"])
+    assert np.abs(a["dH"] - b["dH"]).max() < 1e-6
+    assert np.abs(a["plaquette"] - b["plaquette"]).max() < 1e-9
+    assert np.abs(a["L_phi"] - b["L_phi"]).max() < 1e-9
