@@ -19,6 +19,9 @@ using namespace ghk;
 namespace {
 thread_local std::string g_err;
 }
+namespace ghpot {
+void set_host_error(const std::string& m) { g_err = m; }
+}
 
 struct gh_ctx {
   int D = 0, N = 0, ng = 0, nlat = 0, prec = 0, rep = 0, d = 0, real = 0, scalar = 0;
@@ -110,6 +113,7 @@ void invalidate_graph(gh_ctx* ctx) {
 void enq_kick(gh_ctx* ctx, double eps) {
   if (ctx->rep == REP_GEN) ctx->eng->gen_links(ctx->b, eps, 0, nullptr);
   ctx->eng->kick(ctx->b, eps, M_UPDATE, F_GAUGE | F_MATTER, nullptr, true, true);
+  if (ctx->b.frozen) ctx->eng->sphere(ctx->b, 0);   // drop the radial force (src/hmc/gauge_higgs_hmc.hpp:133)
 }
 void enq_drift(gh_ctx* ctx, double eps) { ctx->eng->drift(ctx->b, eps, ctx->prec == GH_PREC_FP32_MD ? 1 : 0); }
 
@@ -180,6 +184,7 @@ void enq_trajectory(gh_ctx* ctx) {
   InitArgs ia{};
   ia.what = 1; ia.pure = ctx->scalar ? 0 : 1; ia.real = ctx->real; ia.d = ctx->d; ia.vec = b.pi;
   ctx->eng->init(b, ia, true, ctx->scalar != 0);
+  if (b.frozen) ctx->eng->sphere(b, 0);   // tangent-space momenta (src/hmc/gauge_higgs_hmc.hpp:172)
   cudaMemcpyAsync(b.Us, b.U, (size_t)ctx->nU * 2 * ctx->rs, cudaMemcpyDeviceToDevice, ctx->st);
   if (ctx->scalar) cudaMemcpyAsync(b.phis, b.phi, (size_t)ctx->nF * 2 * ctx->rs, cudaMemcpyDeviceToDevice, ctx->st);
   enq_measure(ctx, 0);
@@ -410,10 +415,6 @@ int build_general(gh_ctx* ctx, const gh_rep_desc* r) {
 extern "C" {
 
 const char* gh_last_error(const gh_ctx* ctx) { return ctx ? ctx->err.c_str() : g_err.c_str(); }
-
-namespace ghpot {
-void set_host_error(const std::string& m) { g_err = m; }
-}
 
 uint64_t gh_rng_key(uint64_t a, uint64_t b, uint64_t c, uint64_t d, uint64_t e) { return ghrng::key(a, b, c, d, e); }
 double gh_rng_uniform(uint64_t seed, uint64_t key) { return ghrng::uniform(seed, key); }
@@ -693,7 +694,25 @@ int gh_refresh_momenta(gh_ctx* ctx) {
   InitArgs a{};
   a.what = 1; a.pure = ctx->scalar ? 0 : 1; a.real = ctx->real; a.d = ctx->d; a.vec = ctx->b.pi;
   ctx->eng->init(ctx->b, a, true, ctx->scalar != 0);
+  if (ctx->b.frozen) ctx->eng->sphere(ctx->b, 0);
   return launch_check(ctx, "refresh_momenta");
+}
+
+// Frozen-length scalar |phi_x| = 1 (GaugeHiggsHMC::frozen_phi, normalize_phi;
+// src/hmc/gauge_higgs_hmc.hpp:38-40,61-103).
+int gh_set_frozen_phi(gh_ctx* ctx, int on) {
+  if (!ctx) return fail(nullptr, GH_ERR_ARG, "null context");
+  if (on && !ctx->scalar) return fail(ctx, GH_ERR_STATE, "no scalar field in a pure-gauge context");
+  CK(cudaStreamSynchronize(ctx->st));
+  ctx->b.frozen = on ? 1 : 0;
+  invalidate_graph(ctx);
+  return GH_OK;
+}
+int gh_normalize_phi(gh_ctx* ctx) {
+  if (!ctx) return fail(nullptr, GH_ERR_ARG, "null context");
+  if (!ctx->scalar) return fail(ctx, GH_ERR_STATE, "no scalar field in a pure-gauge context");
+  ctx->eng->sphere(ctx->b, 1);
+  return launch_check(ctx, "normalize_phi");
 }
 
 int gh_gauge_force(gh_ctx* ctx, int lat, double* F) {

@@ -23,6 +23,7 @@ struct Bufs {
   int hist_cap;
   GenTables gen;
   int nlat, D, N, d, rep, scalar;
+  int frozen;            // frozen-length scalar |phi_x| = 1
   int pot;               // POT_QUARTIC or POT_MULTI
   double mu2;
   const double2* asup64; // multi-invariant potential superoperator, FP64 and FP32 copies
@@ -36,6 +37,7 @@ struct EngineBase {
   virtual void gen_links(const Bufs& b, double eps, int mode, double* out) = 0;
   virtual void drift(const Bufs& b, double eps, int reunit) = 0;
   virtual void reunit(const Bufs& b) = 0;
+  virtual void sphere(const Bufs& b, int what) = 0;
   virtual void measure(const Bufs& b) = 0;
   virtual void init(const Bufs& b, InitArgs a, bool links, bool sites) = 0;
   virtual void restore(const Bufs& b) = 0;
@@ -81,8 +83,14 @@ struct Engine : EngineBase {
   void drift(const Bufs& b, double eps, int reunit) override {
     DriftArgs a;
     a.work = b.w_all; a.lats = b.lats; a.U = b.U; a.P = b.P; a.phi = b.phi; a.pi = b.pi;
-    a.eps = eps; a.reunit = reunit; a.d = b.d;
+    a.eps = eps; a.reunit = reunit; a.d = b.d; a.frozen = b.frozen;
     k_drift<N, R><<<b.nw_links + (b.scalar ? b.nw_sites : 0), KBLOCK, 0, b.st>>>(a);
+  }
+  void sphere(const Bufs& b, int what) override {
+    if (!b.scalar) return;
+    SphereArgs a;
+    a.work = b.w_all + b.nw_links; a.lats = b.lats; a.phi = b.phi; a.pi = b.pi; a.d = b.d; a.what = what;
+    k_sphere<R><<<b.nw_sites, KBLOCK, 0, b.st>>>(a);
   }
   void reunit(const Bufs& b) override {
     LinkArgs a;

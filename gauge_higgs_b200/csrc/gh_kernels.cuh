@@ -621,10 +621,11 @@ struct DriftArgs {
   void* U;
   const void* P;
   void* phi;
-  const void* pi;
+  void* pi;
   double eps;
   int reunit;
   int d;
+  int frozen;          // |phi_x| = 1: geodesic (great-circle) drift of (phi, pi)
 };
 template <int N, typename R>
 __global__ void __launch_bounds__(KBLOCK) k_drift(const DriftArgs a) {
@@ -647,6 +648,37 @@ __global__ void __launch_bounds__(KBLOCK) k_drift(const DriftArgs a) {
     Mat<N, R> Un = mm(E, ld_link_rw<N, R>((const R*)a.U, L, mu, s));
     if (a.reunit) project_su<N, R>(Un);
     st_link<N, R>((R*)a.U, L, mu, s, Un);
+  } else if (a.frozen) {
+    // Frozen length (src/hmc/gauge_higgs_hmc.hpp:84-102): the exact constrained free
+    // flow on the unit sphere, r = |pi|:
+    //   phi' = cos(r eps) phi + sin(r eps) pi / r,  pi' = -r sin(r eps) phi + cos(r eps) pi.
+    // FP64 arithmetic in both precisions; FP32 fields are put back on the sphere
+    // (phi' / |phi'|) before they are stored, so that FP32 rounding does not let
+    // |phi| wander over many steps.
+    R* phi = (R*)a.phi;
+    R* pi = (R*)a.pi;
+    double r2 = 0.0;
+    for (int k = 0; k < a.d; ++k) r2 += norm2(ldc_rw<double>(pi, f_index(L, a.d, k, s)));
+    const double r = sqrt(r2);
+    if (r < 1e-300) return;
+    double sn, c;
+    sincos(r * a.eps, &sn, &c);
+    const double sr = sn / r, rs = -r * sn;
+    double inv = 1.0;
+    if (sizeof(R) != sizeof(double)) {
+      double n2 = 0.0;
+      for (int k = 0; k < a.d; ++k) {
+        const long long i = f_index(L, a.d, k, s);
+        n2 += norm2(add(scale(ldc_rw<double>(phi, i), c), scale(ldc_rw<double>(pi, i), sr)));
+      }
+      inv = 1.0 / sqrt(n2);
+    }
+    for (int k = 0; k < a.d; ++k) {
+      const long long i = f_index(L, a.d, k, s);
+      const cx<double> f = ldc_rw<double>(phi, i), p = ldc_rw<double>(pi, i);
+      stc<double>(phi, i, scale(add(scale(f, c), scale(p, sr)), inv));
+      stc<double>(pi, i, add(scale(f, rs), scale(p, c)));
+    }
   } else {
     typedef typename Cmp<R>::t C;
     R* phi = (R*)a.phi;
@@ -654,6 +686,44 @@ __global__ void __launch_bounds__(KBLOCK) k_drift(const DriftArgs a) {
     for (int k = 0; k < a.d; ++k) {
       const long long i = f_index(L, a.d, k, s);
       stc<C>(phi, i, add(ldc_rw<C>(phi, i), scale(ldc<C>(pi, i), (C)a.eps)));
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Frozen-length scalar helpers, one thread per site (src/hmc/gauge_higgs_hmc.hpp:61-82):
+//   what 0: pi <- pi - Re(phi^dag pi) phi   (momentum onto the sphere's tangent space)
+//   what 1: phi <- phi / |phi|              (put the field on the unit sphere)
+// FP64 arithmetic in both precisions.
+// ---------------------------------------------------------------------------
+struct SphereArgs { const Work* work; const LatDev* lats; void* phi; void* pi; int d; int what; };
+template <typename R>
+__global__ void __launch_bounds__(KBLOCK) k_sphere(const SphereArgs a) {
+  const Work w = a.work[blockIdx.x];
+  if ((int)threadIdx.x >= w.n) return;
+  const LatDev& L = a.lats[w.lat];
+  const int s = w.s0 + threadIdx.x;
+  R* phi = (R*)a.phi;
+  R* pi = (R*)a.pi;
+  if (a.what == 0) {
+    double rp = 0.0;
+    for (int k = 0; k < a.d; ++k) {
+      const long long i = f_index(L, a.d, k, s);
+      const cx<double> f = ldc_rw<double>(phi, i), p = ldc_rw<double>(pi, i);
+      rp += f.re * p.re + f.im * p.im;
+    }
+    for (int k = 0; k < a.d; ++k) {
+      const long long i = f_index(L, a.d, k, s);
+      stc<double>(pi, i, sub(ldc_rw<double>(pi, i), scale(ldc_rw<double>(phi, i), rp)));
+    }
+  } else {
+    double n2 = 0.0;
+    for (int k = 0; k < a.d; ++k) n2 += norm2(ldc_rw<double>(phi, f_index(L, a.d, k, s)));
+    if (!(n2 > 0.0)) return;
+    const double inv = 1.0 / sqrt(n2);
+    for (int k = 0; k < a.d; ++k) {
+      const long long i = f_index(L, a.d, k, s);
+      stc<double>(phi, i, scale(ldc_rw<double>(phi, i), inv));
     }
   }
 }

@@ -5,7 +5,8 @@
 //   hmc_higgs_multi <rep> <L> <beta> <kappa> <mu2> <couplings|auto> [ntherm=80 nmeas=200 nmd=24 tau=1 seed=1 ts_outfile]
 //     <couplings> = comma list f_0,f_1,... in the printed channel (C2) order, or "auto" (all 1)
 //   Run with just <rep> to print the channels.  GH_COLD=1: ordered start (identity
-//   links, phi = (1, 0, ...)) instead of hot.  GH_PRECISION=fp32: FP32-MD mode.
+//   links, phi = (1, 0, ...)) instead of hot.  GH_FROZEN=1: frozen-length scalar
+//   |phi_x| = 1.  GH_PRECISION=fp32: FP32-MD mode.
 // Compile-time D = NDIM, N = NCOL as in the reference build.
 #include <cstdio>
 #include <cstdlib>
@@ -56,10 +57,7 @@ int main(int argc, char** argv) {
       std::fprintf(stderr, "error: need %d couplings, got %zu\n", ch.n_channels(), f.size());
       return 1;
     }
-    if (std::getenv("GH_FROZEN")) {
-      std::fprintf(stderr, "error: the frozen-length scalar (GH_FROZEN) is not supported by this engine\n");
-      return 1;
-    }
+    const bool frozen = std::getenv("GH_FROZEN") != nullptr;   // |phi_x| = 1 frozen-length scalar
     const char* pe = std::getenv("GH_PRECISION");
     const ghb::Precision prec = (pe && std::strcmp(pe, "fp32") == 0) ? ghb::Precision::FP32_MD : ghb::Precision::FP64;
     ghb::MultiInvariantPotential<kN> pot(ch, f, mu2);
@@ -68,10 +66,12 @@ int main(int argc, char** argv) {
     for (int mu = 0; mu < kDim; ++mu) L[mu] = Lext;
     ghb::GaugeHiggsHMC<kDim, kN> hmc(L, rep, seed, prec);
     hmc.beta = beta; hmc.kappa = kappa; hmc.tau = tau; hmc.nmd = nmd; hmc.potential = &pot;
-    std::printf("# D=%d SU(%d) L=%d^%d  beta=%.3f kappa=%.3f mu2=%.3f nmd=%d  potential=multi-invariant\n", kDim, kN, Lext,
-                kDim, beta, kappa, mu2, nmd);
+    hmc.frozen_phi = frozen;
+    std::printf("# D=%d SU(%d) L=%d^%d  beta=%.3f kappa=%.3f mu2=%.3f nmd=%d  potential=multi-invariant%s\n", kDim, kN,
+                Lext, kDim, beta, kappa, mu2, nmd, frozen ? "  [FROZEN |phi|=1]" : "");
     if (std::getenv("GH_COLD")) { hmc.cold(); hmc.phi_cold(1.0); }
     else { hmc.hot(0.8); hmc.phi_gaussian(12345, 0.3); }
+    if (frozen) hmc.normalize_phi();   // onto |phi_x| = 1 before thermalising
     hmc.run(ntherm);
 
     hmc.traj_count = 0; hmc.accept_count = 0;

@@ -250,6 +250,22 @@ class Ensemble:
             self.ctx("gh_set_potential_multi", len(pot.f), _dptr(pot.f), pot.mu2)
         self._potential = pot
 
+    # ---- frozen-length scalar ----
+    @property
+    def frozen_phi(self):
+        return getattr(self, "_frozen", False)
+
+    @frozen_phi.setter
+    def frozen_phi(self, on):
+        """GaugeHiggsHMC::frozen_phi (src/hmc/gauge_higgs_hmc.hpp:38-40): |phi_x| = 1
+        HMC with tangent-space momenta and the great-circle scalar drift."""
+        self.ctx("gh_set_frozen_phi", 1 if on else 0)
+        self._frozen = bool(on)
+
+    def normalize_phi(self):
+        """Put every site on the unit sphere (src/hmc/gauge_higgs_hmc.hpp:73-82)."""
+        self.ctx("gh_normalize_phi")
+
     # ---- couplings / integrator ----
     def set_couplings(self, lat, beta, kappa, lam):
         self.ctx("gh_set_couplings", lat, beta, kappa, lam)

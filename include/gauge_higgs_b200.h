@@ -293,6 +293,16 @@ int gh_multi_superop(int N, const gh_rep_desc* rep, int n_channels, const double
 int gh_set_potential_multi(gh_ctx* ctx, int n_channels, const double* f, double mu2);
 int gh_set_potential_quartic(gh_ctx* ctx);
 
+/* ---- frozen-length scalar, |phi_x| = 1 ----
+ * Replaces GaugeHiggsHMC::frozen_phi and normalize_phi (src/hmc/gauge_higgs_hmc.hpp:
+ * 38-40,61-103): with it on, momenta are projected onto the tangent space of each
+ * site's unit sphere after every refresh and kick, and the scalar drift is the exact
+ * great-circle flow.  gh_normalize_phi puts every site on the sphere (call once
+ * after the initial field, as the reference drivers do).  Both stream-ordered;
+ * gh_set_frozen_phi invalidates a captured trajectory graph. */
+int gh_set_frozen_phi(gh_ctx* ctx, int on);
+int gh_normalize_phi(gh_ctx* ctx);
+
 #ifdef __cplusplus
 }
 #endif

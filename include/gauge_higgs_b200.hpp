@@ -127,6 +127,7 @@ class GaugeHiggsHMC {
   int64_t vol = 1;
   // optional onsite potential (src/hmc/gauge_higgs_hmc.hpp:25-27); nullptr = quartic in lambda
   const MultiInvariantPotential<N>* potential = nullptr;
+  bool frozen_phi = false;   // |phi_x| = 1 scalar (src/hmc/gauge_higgs_hmc.hpp:38-40)
 
   GaugeHiggsHMC(const std::array<int, D>& extents, const Representation& R, std::uint64_t seed,
                 Precision prec = Precision::FP64)
@@ -147,6 +148,7 @@ class GaugeHiggsHMC {
   void cold() { check(gh_cold_start(ctx_), ctx_); }
   void phi_gaussian(std::uint64_t stream, double sigma = 1.0) { check(gh_phi_gaussian(ctx_, stream, sigma), ctx_); }
   void phi_cold(double c = 1.0) { check(gh_phi_cold(ctx_, c), ctx_); }
+  void normalize_phi() { check(gh_normalize_phi(ctx_), ctx_); }
 
   void kick(double eps) { sync_params(); check(gh_kick(ctx_, eps), ctx_); }
   void drift(double eps) { sync_params(); check(gh_drift(ctx_, eps), ctx_); }
@@ -222,6 +224,10 @@ class GaugeHiggsHMC {
       check(gh_set_traj_count(ctx_, 0, traj_count, accept_count), ctx_);
       ptc_ = traj_count; pac_ = accept_count;
     }
+    if (frozen_phi != pfz_) {
+      check(gh_set_frozen_phi(ctx_, frozen_phi ? 1 : 0), ctx_);
+      pfz_ = frozen_phi;
+    }
     if (potential != ppot_) {
       if (potential) check(gh_set_potential_multi(ctx_, (int)potential->f.size(), potential->f.data(), potential->mu2), ctx_);
       else check(gh_set_potential_quartic(ctx_), ctx_);
@@ -241,6 +247,7 @@ class GaugeHiggsHMC {
   int pn_ = -1, pi_ = -1;
   std::uint64_t ptc_ = 0, pac_ = 0;
   const MultiInvariantPotential<N>* ppot_ = nullptr;
+  bool pfz_ = false;
 };
 
 template <int D, int N>

@@ -397,6 +397,9 @@ class Reference:
         L.ref_scalar_action.restype = C.c_double
         L.ref_scalar_action.argtypes = [C.c_int, C.c_int, _ip, C.c_char_p, _dp, _dp, C.c_double, C.c_double]
         L.ref_casimir_channels.argtypes = [C.c_int, C.c_char_p, _dp, C.c_int]
+        L.ref_hmc_op_frozen.argtypes = [C.c_int, C.c_int, C.c_int, _ip, C.c_char_p, _u64, C.c_double, C.c_double,
+                                        C.c_double, C.c_double, C.c_int, C.c_int, C.c_double, _u64, _dp, _dp, _dp,
+                                        _dp, _dp]
         L.ref_multi_superop.argtypes = [C.c_int, C.c_char_p, _dp, C.c_int, C.c_double, _dp]
         L.ref_multi_value_dV.argtypes = [C.c_int, C.c_char_p, _dp, C.c_int, C.c_double, _dp, _dp, _dp]
         L.ref_scalar_force_multi.argtypes = [C.c_int, C.c_int, _ip, C.c_char_p, _dp, _dp, C.c_double, _dp, C.c_int,
@@ -609,6 +612,20 @@ class Reference:
                                  eps, traj_count, _d(U), _d(P), _d(phi), _d(pi), _d(out))
         if rc:
             raise RuntimeError(f"ref_hmc_op rc={rc}")
+        state.update(st)
+        return out
+
+    def hmc_op_frozen(self, op, D, N, L, spec, state, seed=1, beta=2.3, kappa=0.1, lam=0.5, tau=1.0, nmd=20,
+                      integ=OMELYAN, eps=0.0, traj_count=0):
+        """As hmc_op with GaugeHiggsHMC::frozen_phi on; op also "normalize"."""
+        ops = dict(kick=0, drift=1, md_evolve=2, hamiltonian=3, refresh=4, trajectory=5, normalize=7)
+        out = np.zeros(4)
+        st = {k: np.ascontiguousarray(v) for k, v in state.items()}
+        rc = self.lib.ref_hmc_op_frozen(ops[op], D, N, self._L(L), spec.encode(), seed, beta, kappa, lam, tau, nmd,
+                                        integ, eps, traj_count, _d(st["U"].view(np.float64)), _d(st["P"]),
+                                        _d(st["phi"].view(np.float64)), _d(st["pi"].view(np.float64)), _d(out))
+        if rc:
+            raise RuntimeError(f"ref_hmc_op_frozen rc={rc}")
         state.update(st)
         return out
 

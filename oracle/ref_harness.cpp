@@ -301,6 +301,25 @@ int ref_hmc_op(int op, int D, int N, const int* L, const char* spec, uint64_t se
 #undef CALL
 }
 
+// Frozen-length scalar (GaugeHiggsHMC::frozen_phi = true): op 0 kick, 1 drift,
+// 2 md_evolve, 3 hamiltonian, 4 refresh_momenta, 5 trajectory, 7 normalize_phi.
+int ref_hmc_op_frozen(int op, int D, int N, const int* L, const char* spec, uint64_t seed,
+                      double beta, double kappa, double lambda, double tau, int nmd, int integ,
+                      double eps, uint64_t traj_count, double* U, double* P, double* phi, double* pi, double* out) {
+#define CALL(DD, NN) { \
+    auto* r = get_rep<NN>(spec); if (!r) return -2; \
+    GaugeHiggsHMC<DD, NN> h(ext<DD>(L), *r, seed); h.beta = beta; h.kappa = kappa; h.lambda = lambda; h.tau = tau; h.nmd = nmd; \
+    h.integ = integ == 0 ? Integrator::Leapfrog : Integrator::Omelyan2MN; h.traj_count = traj_count; h.frozen_phi = true; \
+    load_U(h.U, U); load_P(h.P, P); load_V(h.phi, phi); load_V(h.pi, pi); \
+    switch (op) { case 0: h.kick(eps); break; case 1: h.drift(eps); break; case 2: h.md_evolve(); break; \
+      case 3: out[0] = h.hamiltonian(); break; case 4: h.refresh_momenta(); break; \
+      case 5: { bool a = h.trajectory(); out[0] = h.last_dH; out[1] = a; out[2] = (double)h.traj_count; break; } \
+      case 7: h.normalize_phi(); break; default: return -3; } \
+    store_U(h.U, U); store_P(h.P, P); store_V(h.phi, phi); store_V(h.pi, pi); return 0; }
+  DISPATCH_DN(D, N, CALL)
+#undef CALL
+}
+
 // ---- the driver loop of src/hmc_higgs.cpp:64-87 / src/main.cpp:26-42 ----
 // series: [nmeas][5] = plaquette, L_phi, L_link, Polyakov, dH (pure gauge: L_phi = L_link = 0)
 // U0/phi0: optional start configuration (null => hot(hot_sigma) and gaussian(12345, phi_sigma))

@@ -165,9 +165,41 @@ def multi_fixture():
     np.savez_compressed(os.path.join(HERE, "multi_potential.npz"), **out)
 
 
+def frozen_fixture():
+    """Frozen-length scalar (GaugeHiggsHMC::frozen_phi): normalize_phi, the tangent-space
+    refresh, one kick (radial force dropped), one geodesic drift and a whole MD evolution
+    of the reference, from one start state."""
+    out = {}
+    for name, D, N, L, spec, kappa in [("su2_fund", 3, 2, [3, 4, 2], "fund", 0.3), ("su3_adj", 3, 3, [2, 3, 2], "adj", 0.2),
+                                       ("su2_spin3", 2, 2, [3, 2], "6", 0.25)]:
+        d = {"fund": N, "adj": N * N - 1}.get(spec) or R.rep_info(N, spec)["d"]
+        V = int(np.prod(L))
+        st = {"U": R.hot_start(D, N, L, 3, 0.6), "P": np.zeros((V, D, N * N - 1)),
+              "phi": R.phi_gaussian(D, L, d, 3, 12345, spec == "adj", 0.7), "pi": np.zeros((V, d), np.complex128)}
+        kw = dict(seed=3, beta=2.1, kappa=kappa, lam=0.5, nmd=3, tau=0.5, integ=OMELYAN)
+        R.hmc_op_frozen("normalize", D, N, L, spec, st, **kw)
+        out[name + "_U0"], out[name + "_phi0"], out[name + "_L"] = st["U"].copy(), st["phi"].copy(), np.array(L)
+        R.hmc_op_frozen("refresh", D, N, L, spec, st, **kw)
+        out[name + "_P0"], out[name + "_pi0"] = st["P"].copy(), st["pi"].copy()
+        s1 = {k: v.copy() for k, v in st.items()}
+        R.hmc_op_frozen("kick", D, N, L, spec, s1, eps=0.07, **kw)
+        out[name + "_kick_P"], out[name + "_kick_pi"] = s1["P"], s1["pi"]
+        s2 = {k: v.copy() for k, v in st.items()}
+        R.hmc_op_frozen("drift", D, N, L, spec, s2, eps=0.07, **kw)
+        out[name + "_drift_U"], out[name + "_drift_phi"], out[name + "_drift_pi"] = s2["U"], s2["phi"], s2["pi"]
+        s3 = {k: v.copy() for k, v in st.items()}
+        R.hmc_op_frozen("md_evolve", D, N, L, spec, s3, **kw)
+        out[name + "_md_U"], out[name + "_md_phi"], out[name + "_md_pi"] = s3["U"], s3["phi"], s3["pi"]
+        out[name + "_H0"] = R.hmc_op_frozen("hamiltonian", D, N, L, spec, {k: v.copy() for k, v in st.items()}, **kw)[0]
+    np.savez_compressed(os.path.join(HERE, "frozen_phi.npz"), **out)
+
+
 if __name__ == "__main__" and sys.argv[1:] == ["multi"]:
     multi_fixture()
+elif __name__ == "__main__" and sys.argv[1:] == ["frozen"]:
+    frozen_fixture()
 elif __name__ == "__main__":
+    frozen_fixture()
     multi_fixture()
     rng_fixture()
     rep_fixture()
