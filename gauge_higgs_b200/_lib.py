@@ -100,6 +100,8 @@ SIGNATURES = {
     "gh_set_potential_multi": [_ctx, C.c_int, _dp, C.c_double],
     "gh_set_potential_quartic": [_ctx],
     "gh_set_frozen_phi": [_ctx, C.c_int],
+    "gh_wilson_loop": [_ctx, C.c_int, C.c_int, C.c_int, _ip, C.c_int, _dp],
+    "gh_polyakov_rep": [_ctx, C.c_int, C.c_int, _ip, C.c_int, _dp],
     "gh_normalize_phi": [_ctx],
     "gh_plaquette_noalloc": [C.c_int, C.c_int, _ip, C.c_void_p, C.c_void_p, C.c_void_p],
     "gh_mlp_create": [C.c_int, _ip, C.c_int, C.c_uint64, C.POINTER(C.c_void_p)],

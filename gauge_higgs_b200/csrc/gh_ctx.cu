@@ -783,6 +783,85 @@ int gh_measure(gh_ctx* ctx, int lat, gh_obs* out) {
   return GH_OK;
 }
 
+// Per-lattice sums of the per-block partials written by a site-item reduction
+// kernel (site items are laid out per lattice in order), divided by norm[l].
+int site_partials_to_lattices(gh_ctx* ctx, int lat, const std::vector<double>& norm, double* out) {
+  std::vector<double> part(ctx->b.nw_sites);
+  CK(cudaMemcpyAsync(part.data(), ctx->b.partials, part.size() * sizeof(double), cudaMemcpyDeviceToHost, ctx->st));
+  CK(cudaStreamSynchronize(ctx->st));
+  int first = 0;
+  const int l0 = lat < 0 ? 0 : lat, l1 = lat < 0 ? ctx->nlat : lat + 1;
+  for (int l = 0; l < ctx->nlat; ++l) {
+    const int nb = (ctx->lat_h[l].V + KBLOCK - 1) / KBLOCK;
+    if (l >= l0 && l < l1) {
+      double sum = 0.0;
+      for (int q = first; q < first + nb; ++q) sum += part[q];
+      out[l - l0] = sum / norm[l];
+    }
+    first += nb;
+  }
+  return GH_OK;
+}
+
+// Probe irrep of a traced loop from its Young rows (NULL: the fundamental); its
+// dimension by the hook-content formula d = prod_cells (N + col - row) / hook.
+int probe_rep(gh_ctx* ctx, const int* rows, int nrows, LoopArgs& a, double& d) {
+  if (!rows || nrows == 0) { a.m = 1; a.lam[0] = 1; d = ctx->N; return GH_OK; }
+  if (nrows < 0 || nrows > CHAR_MMAX || nrows > ctx->N) return fail(ctx, GH_ERR_ARG, "probe irrep: 1 to N Young rows");
+  for (int i = 0; i < nrows; ++i)
+    if (rows[i] < 1 || (i > 0 && rows[i] > rows[i - 1])) return fail(ctx, GH_ERR_ARG, "probe irrep: Young rows must be positive and non-increasing");
+  if (rows[0] + nrows - 1 > CHAR_KMAX) return fail(ctx, GH_ERR_UNSUPPORTED, "probe irrep: first row too long");
+  a.m = nrows;
+  double num = 1.0, den = 1.0;
+  for (int i = 0; i < nrows; ++i) {
+    a.lam[i] = rows[i];
+    for (int j = 0; j < rows[i]; ++j) {
+      int below = 0;
+      for (int k = i + 1; k < nrows; ++k) below += rows[k] > j;
+      num *= (double)(ctx->N + j - i);
+      den *= (double)(rows[i] - j - 1 + below + 1);
+    }
+  }
+  d = num / den;
+  return GH_OK;
+}
+
+// Wilson loops W(Ra, Rb) traced in a probe irrep, averaged over sites and planes
+// mu < nu (wilson_loop_fund / wilson_loop_rep, src/measure/observables.hpp:48-79);
+// Polyakov loops traced in a probe irrep (polyakov_loop_rep, :81-101).
+int gh_wilson_loop(gh_ctx* ctx, int lat, int Ra, int Rb, const int* rows, int nrows, double* out) {
+  int rc = check_lat(ctx, lat, true);
+  if (rc) return rc;
+  if (!out) return fail(ctx, GH_ERR_ARG, "null output");
+  if (Ra < 1 || Rb < 1) return fail(ctx, GH_ERR_ARG, "loop extents must be >= 1");
+  LoopArgs a{};
+  double d = 0.0;
+  if ((rc = probe_rep(ctx, rows, nrows, a, d))) return rc;
+  a.mode = 1; a.Ra = Ra; a.Rb = Rb;
+  ctx->eng->loops(ctx->b, a);
+  if ((rc = launch_check(ctx, "wilson_loop"))) return rc;
+  std::vector<double> norm(ctx->nlat);
+  for (int l = 0; l < ctx->nlat; ++l) norm[l] = (double)ctx->lat_h[l].V * (ctx->D * (ctx->D - 1) / 2) * d;
+  return site_partials_to_lattices(ctx, lat, norm, out);
+}
+
+int gh_polyakov_rep(gh_ctx* ctx, int lat, int tdir, const int* rows, int nrows, double* out) {
+  int rc = check_lat(ctx, lat, true);
+  if (rc) return rc;
+  if (!out) return fail(ctx, GH_ERR_ARG, "null output");
+  if (tdir < 0) tdir = ctx->D - 1;
+  if (tdir >= ctx->D) return fail(ctx, GH_ERR_ARG, "tdir out of range");
+  LoopArgs a{};
+  double d = 0.0;
+  if ((rc = probe_rep(ctx, rows, nrows, a, d))) return rc;
+  a.mode = 0; a.tdir = tdir;
+  ctx->eng->loops(ctx->b, a);
+  if ((rc = launch_check(ctx, "polyakov_rep"))) return rc;
+  std::vector<double> norm(ctx->nlat);
+  for (int l = 0; l < ctx->nlat; ++l) norm[l] = (double)ctx->lat_h[l].V / ctx->lat_h[l].L[tdir] * d;
+  return site_partials_to_lattices(ctx, lat, norm, out);
+}
+
 int gh_polyakov(gh_ctx* ctx, int lat, int tdir, double* out) {
   int rc = check_lat(ctx, lat, true);
   if (rc) return rc;

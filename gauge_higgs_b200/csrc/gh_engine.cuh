@@ -42,6 +42,7 @@ struct EngineBase {
   virtual void init(const Bufs& b, InitArgs a, bool links, bool sites) = 0;
   virtual void restore(const Bufs& b) = 0;
   virtual void polyakov(const Bufs& b, int tdir) = 0;
+  virtual void loops(const Bufs& b, LoopArgs a) = 0;
   virtual void xfer(const Bufs& b, XferArgs a) = 0;
   virtual size_t gen_smem(const Bufs& b) const = 0;
   virtual int prepare(const Bufs& b) = 0;
@@ -122,6 +123,10 @@ struct Engine : EngineBase {
     PolyArgs a;
     a.work = b.w_all + b.nw_links; a.lats = b.lats; a.U = b.U; a.tdir = tdir; a.partials = b.partials;
     k_polyakov<D, N, R><<<b.nw_sites, KBLOCK, 0, b.st>>>(a);
+  }
+  void loops(const Bufs& b, LoopArgs a) override {
+    a.work = b.w_all + b.nw_links; a.lats = b.lats; a.U = b.U; a.partials = b.partials;
+    k_loops<D, N, R><<<b.nw_sites, KBLOCK, 0, b.st>>>(a);
   }
   void xfer(const Bufs& b, XferArgs a) override {
     a.lats = b.lats;

@@ -1079,6 +1079,130 @@ __global__ void __launch_bounds__(KBLOCK) k_polyakov(const PolyArgs a) {
 }
 
 // ---------------------------------------------------------------------------
+// Loops traced in a probe irrep (src/measure/observables.hpp:36-101).
+// Re chi_lambda(W) for an SU(N) matrix W and Young rows lambda (m rows): the Schur
+// polynomial of W's eigenvalues by Jacobi-Trudi, s_lambda = det[h_{lambda_i - i + j}],
+// with the complete symmetric polynomials h_k from the power sums p_k = Tr W^k by
+// Newton's identities, k h_k = sum_{i=1}^{k} p_i h_{k-i}.  This is Tr D^(lambda)(W),
+// the trace of the representation matrix, without forming it.
+// ---------------------------------------------------------------------------
+constexpr int CHAR_KMAX = 24;     // largest h index lambda_1 + m - 1
+constexpr int CHAR_MMAX = 4;      // most Young rows
+
+template <int N>
+__device__ double re_character(const Mat<N, double>& W, const int* lam, int m) {
+  const int K = lam[0] + m - 1;
+  cx<double> p[CHAR_KMAX + 1], h[CHAR_KMAX + 1];
+  Mat<N, double> Wk = W;
+  for (int k = 1; k <= K; ++k) {
+    if (k > 1) Wk = mm(Wk, W);
+    cx<double> t = zero<double>();
+    for (int i = 0; i < N; ++i) t = add(t, Wk.e[i * N + i]);
+    p[k] = t;
+  }
+  h[0] = mk<double>(1.0, 0.0);
+  for (int k = 1; k <= K; ++k) {
+    cx<double> t = zero<double>();
+    for (int i = 1; i <= k; ++i) t = cfma(t, p[i], h[k - i]);
+    h[k] = scale(t, 1.0 / k);
+  }
+  cx<double> M[CHAR_MMAX * CHAR_MMAX];
+  for (int i = 0; i < m; ++i)
+    for (int j = 0; j < m; ++j) {
+      const int k = lam[i] - i + j;
+      M[i * m + j] = (k < 0) ? zero<double>() : h[k];
+    }
+  // determinant by elimination with partial pivoting (m <= 4)
+  cx<double> det = mk<double>(1.0, 0.0);
+  for (int c = 0; c < m; ++c) {
+    int piv = c;
+    for (int r = c + 1; r < m; ++r)
+      if (norm2(M[r * m + c]) > norm2(M[piv * m + c])) piv = r;
+    if (norm2(M[piv * m + c]) == 0.0) return 0.0;
+    if (piv != c) {
+      for (int j = 0; j < m; ++j) { const cx<double> t = M[c * m + j]; M[c * m + j] = M[piv * m + j]; M[piv * m + j] = t; }
+      det = scale(det, -1.0);
+    }
+    det = mul(det, M[c * m + c]);
+    const cx<double> inv = scale(conj(M[c * m + c]), 1.0 / norm2(M[c * m + c]));
+    for (int r = c + 1; r < m; ++r) {
+      const cx<double> f = mul(M[r * m + c], inv);
+      for (int j = c; j < m; ++j) M[r * m + j] = sub(M[r * m + j], mul(f, M[c * m + j]));
+    }
+  }
+  return det.re;
+}
+
+// mode 0: Polyakov line in direction tdir from every site with x_tdir = 0;
+// mode 1: the Ra x Rb rectangle of every plane mu < nu based at every site
+//         (path order of wilson_rect, src/measure/observables.hpp:36-46).
+// Per block: sum over its sites of Re chi(loop), into partials (FP64).
+struct LoopArgs {
+  const Work* work; const LatDev* lats; const void* U; double* partials;
+  int mode, tdir, Ra, Rb, m; int lam[CHAR_MMAX];
+};
+template <int D, int N, typename R>
+__global__ void __launch_bounds__(KBLOCK) k_loops(const LoopArgs a) {
+  const Work w = a.work[blockIdx.x];
+  double v = 0.0;
+  if ((int)threadIdx.x < w.n) {
+    const LatDev L = a.lats[w.lat];
+    const int s = w.s0 + threadIdx.x;
+    const R* U = (const R*)a.U;
+    int x0[D];
+    coords<D>(L, s, x0);
+    if (a.mode == 0) {
+      if (x0[a.tdir] == 0) {
+        const int t = a.tdir;
+        Mat<N, double> P = ld_link<N, double>(U, L, t, s);
+        int cur = s, xt = 0;
+        for (int k = 1; k < L.L[t]; ++k) {
+          cur = nfwd(L, cur, xt, t);
+          ++xt;
+          P = mm(P, ld_link<N, double>(U, L, t, cur));
+        }
+        v = re_character<N>(P, a.lam, a.m);
+      }
+    } else {
+      for (int mu = 0; mu < D; ++mu)
+        for (int nu = mu + 1; nu < D; ++nu) {
+          int x[D];
+          for (int q = 0; q < D; ++q) x[q] = x0[q];
+          int c = s;
+          Mat<N, double> W = ld_link<N, double>(U, L, mu, c);
+          c = nfwd(L, c, x[mu], mu); x[mu] = (x[mu] + 1 == L.L[mu]) ? 0 : x[mu] + 1;
+          for (int i = 1; i < a.Ra; ++i) {
+            W = mm(W, ld_link<N, double>(U, L, mu, c));
+            c = nfwd(L, c, x[mu], mu); x[mu] = (x[mu] + 1 == L.L[mu]) ? 0 : x[mu] + 1;
+          }
+          for (int j = 0; j < a.Rb; ++j) {
+            W = mm(W, ld_link<N, double>(U, L, nu, c));
+            c = nfwd(L, c, x[nu], nu); x[nu] = (x[nu] + 1 == L.L[nu]) ? 0 : x[nu] + 1;
+          }
+          for (int i = 0; i < a.Ra; ++i) {
+            c = nbwd(L, c, x[mu], mu); x[mu] = (x[mu] == 0) ? L.L[mu] - 1 : x[mu] - 1;
+            W = mm_nd(W, ld_link<N, double>(U, L, mu, c));
+          }
+          for (int j = 0; j < a.Rb; ++j) {
+            c = nbwd(L, c, x[nu], nu); x[nu] = (x[nu] == 0) ? L.L[nu] - 1 : x[nu] - 1;
+            W = mm_nd(W, ld_link<N, double>(U, L, nu, c));
+          }
+          v += re_character<N>(W, a.lam, a.m);
+        }
+    }
+  }
+  __shared__ double red[KBLOCK / 32];
+  v = warp_sum(v);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0.0;
+    for (int q = 0; q < KBLOCK / 32; ++q) t += red[q];
+    a.partials[blockIdx.x] = t;
+  }
+}
+
+// ---------------------------------------------------------------------------
 // Layout conversion between the reference's AoS host arrays (FP64) and the
 // device SoA planes (R).  kind: 0 links (N*N complex per (site,mu)),
 // 1 momenta (ng reals per (site,mu)), 2 vectors (d complex per site).

@@ -58,6 +58,10 @@ class Representation:
     def name(self):
         return type(self).__name__
 
+    def young_rows(self):
+        """Young rows of the irrep (the probe for traced loops)."""
+        raise NotImplementedError
+
 
 class FundamentalRep(Representation):
     """D(U) = U, d = N (src/rep/rep_fundamental.hpp:15-25)."""
@@ -65,6 +69,9 @@ class FundamentalRep(Representation):
 
     def __init__(self, N):
         super().__init__(N, N)
+
+    def young_rows(self):
+        return [1]
 
     def name(self):
         return "fundamental"
@@ -77,6 +84,9 @@ class AdjointRep(Representation):
 
     def __init__(self, N):
         super().__init__(N, N * N - 1)
+
+    def young_rows(self):
+        return [2] + [1] * (self.N - 2)
 
     def name(self):
         return "adjoint"
@@ -111,6 +121,9 @@ class GeneralRep(Representation):
             spec, tail = spec.split(":", 1)
             real = tail == "real"
         return cls(N, [int(t) for t in spec.split(",") if t], real)
+
+    def young_rows(self):
+        return list(self.rows)
 
     def name(self):
         return "general[" + ",".join(map(str, self.rows)) + "]"
@@ -249,6 +262,28 @@ class Ensemble:
         else:
             self.ctx("gh_set_potential_multi", len(pot.f), _dptr(pot.f), pot.mu2)
         self._potential = pot
+
+    # ---- loops traced in a probe irrep (src/measure/observables.hpp:36-101) ----
+    def _rows(self, rep):
+        if rep is None:
+            return None, 0
+        rows = rep.young_rows() if hasattr(rep, "young_rows") else list(rep)
+        return (C.c_int * len(rows))(*rows), len(rows)
+
+    def wilson_loop(self, Ra, Rb, rep=None, lat=-1):
+        """<(1/d_R) Re Tr D^R(W_loop)> of the Ra x Rb rectangles (wilson_loop_fund when rep is
+        None, wilson_loop_rep otherwise); rep: a Representation or Young rows."""
+        rows, m = self._rows(rep)
+        out = np.zeros(self.n_lat if lat < 0 else 1)
+        self.ctx("gh_wilson_loop", lat, int(Ra), int(Rb), rows, m, _dptr(out))
+        return out if lat < 0 and self.n_lat > 1 else float(out[0])
+
+    def polyakov_loop_rep(self, rep=None, tdir=-1, lat=-1):
+        """<(1/d_R) Re Tr D^R(prod_t U_tdir)> (polyakov_loop_rep)."""
+        rows, m = self._rows(rep)
+        out = np.zeros(self.n_lat if lat < 0 else 1)
+        self.ctx("gh_polyakov_rep", lat, int(tdir), rows, m, _dptr(out))
+        return out if lat < 0 and self.n_lat > 1 else float(out[0])
 
     # ---- frozen-length scalar ----
     @property

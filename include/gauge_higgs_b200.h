@@ -293,6 +293,20 @@ int gh_multi_superop(int N, const gh_rep_desc* rep, int n_channels, const double
 int gh_set_potential_multi(gh_ctx* ctx, int n_channels, const double* f, double mu2);
 int gh_set_potential_quartic(gh_ctx* ctx);
 
+/* ---- loops traced in a probe irrep (src/measure/observables.hpp:36-101) ----
+ * gh_wilson_loop: <(1/d_R) Re Tr D^(R)(W_loop)> over sites and planes mu < nu of
+ *   the Ra x Rb rectangle (wilson_rect :36-46; wilson_loop_fund :48-60 for rows
+ *   = NULL, wilson_loop_rep :62-79 otherwise).
+ * gh_polyakov_rep: <(1/d_R) Re Tr D^(R)(prod_t U_tdir)> (polyakov_loop_rep :81-101);
+ *   tdir < 0 selects D-1.
+ * The probe irrep R is given by its Young rows (rows[0] >= rows[1] >= ... >= 1,
+ * at most N rows, rows[0] + nrows <= 25; NULL: the fundamental).  The trace is the
+ * irrep's character, the same number as the trace of the reference's rep_matrix.
+ * FP64 on the device in both precision modes; one value per lattice into out
+ * (lat = -1: all lattices). */
+int gh_wilson_loop(gh_ctx* ctx, int lat, int Ra, int Rb, const int* rows, int nrows, double* out);
+int gh_polyakov_rep(gh_ctx* ctx, int lat, int tdir, const int* rows, int nrows, double* out);
+
 /* ---- frozen-length scalar, |phi_x| = 1 ----
  * Replaces GaugeHiggsHMC::frozen_phi and normalize_phi (src/hmc/gauge_higgs_hmc.hpp:
  * 38-40,61-103): with it on, momenta are projected onto the tangent space of each

@@ -39,6 +39,7 @@ struct Representation {
   int kind = GH_REP_NONE, N = 0, d = 0, real = 0, n_boxes = 0, nality = 0;
   long dimT = 0;
   std::vector<double> T, W;   // complex interleaved (GENERAL only)
+  std::vector<int> rows;      // Young rows of the irrep
   std::string repname;
   std::string name() const { return repname; }
   gh_rep_desc desc() const {
@@ -51,10 +52,15 @@ struct Representation {
 };
 
 template <int N> Representation FundamentalRep() {
-  Representation r; r.kind = GH_REP_FUND; r.N = N; r.d = N; r.real = 0; r.nality = 1; r.repname = "fundamental"; return r;
+  Representation r; r.kind = GH_REP_FUND; r.N = N; r.d = N; r.real = 0; r.nality = 1; r.repname = "fundamental";
+  r.rows = {1};
+  return r;
 }
 template <int N> Representation AdjointRep() {
-  Representation r; r.kind = GH_REP_ADJ; r.N = N; r.d = N * N - 1; r.real = 1; r.nality = 0; r.repname = "adjoint"; return r;
+  Representation r; r.kind = GH_REP_ADJ; r.N = N; r.d = N * N - 1; r.real = 1; r.nality = 0; r.repname = "adjoint";
+  r.rows.assign((size_t)N - 1, 1);
+  r.rows[0] = 2;
+  return r;
 }
 // GeneralRep<N>(rows, real): the Young-symmetriser irrep (src/rep/rep_general.hpp:54-84)
 template <int N> Representation GeneralRep(std::vector<int> rows, bool real = false) {
@@ -67,6 +73,7 @@ template <int N> Representation GeneralRep(std::vector<int> rows, bool real = fa
   r.W.assign((size_t)r.d * dimT * 2, 0.0);
   check(gh_rep_general_build(N, rows.data(), (int)rows.size(), r.T.data(), r.W.data()), nullptr);
   r.nality = r.n_boxes % N;
+  r.rows = rows;
   r.repname = "general[";
   for (size_t i = 0; i < rows.size(); ++i) r.repname += (i ? "," : "") + std::to_string(rows[i]);
   r.repname += "]";
@@ -182,6 +189,18 @@ class GaugeHiggsHMC {
   double higgs_length() { return measure().L_phi; }
   double link_energy() { return measure().L_link; }
   double polyakov_loop(int tdir = D - 1) { double p; check(gh_polyakov(ctx_, 0, tdir, &p), ctx_); return p; }
+  // loops traced in a probe irrep (src/measure/observables.hpp:48-101)
+  double wilson_loop_fund(int Ra, int Rb) { double w; check(gh_wilson_loop(ctx_, 0, Ra, Rb, nullptr, 0, &w), ctx_); return w; }
+  double wilson_loop_rep(const Representation& R, int Ra, int Rb) {
+    double w;
+    check(gh_wilson_loop(ctx_, 0, Ra, Rb, R.rows.data(), (int)R.rows.size(), &w), ctx_);
+    return w;
+  }
+  double polyakov_loop_rep(const Representation& R, int tdir = D - 1) {
+    double p;
+    check(gh_polyakov_rep(ctx_, 0, tdir, R.rows.data(), (int)R.rows.size(), &p), ctx_);
+    return p;
+  }
 
   // fields in the reference layouts (complex interleaved doubles)
   std::vector<double> U() { std::vector<double> u((size_t)vol * D * N * N * 2); check(gh_get_links(ctx_, 0, u.data()), ctx_); return u; }

@@ -397,6 +397,10 @@ class Reference:
         L.ref_scalar_action.restype = C.c_double
         L.ref_scalar_action.argtypes = [C.c_int, C.c_int, _ip, C.c_char_p, _dp, _dp, C.c_double, C.c_double]
         L.ref_casimir_channels.argtypes = [C.c_int, C.c_char_p, _dp, C.c_int]
+        L.ref_wilson_loop.restype = C.c_double
+        L.ref_wilson_loop.argtypes = [C.c_int, C.c_int, _ip, C.c_char_p, _dp, C.c_int, C.c_int]
+        L.ref_polyakov_rep.restype = C.c_double
+        L.ref_polyakov_rep.argtypes = [C.c_int, C.c_int, _ip, C.c_char_p, _dp, C.c_int]
         L.ref_hmc_op_frozen.argtypes = [C.c_int, C.c_int, C.c_int, _ip, C.c_char_p, _u64, C.c_double, C.c_double,
                                         C.c_double, C.c_double, C.c_int, C.c_int, C.c_double, _u64, _dp, _dp, _dp,
                                         _dp, _dp]
@@ -550,6 +554,13 @@ class Reference:
 
     def scalar_action(self, D, N, L, spec, U, phi, kappa, lam):
         return self.lib.ref_scalar_action(D, N, self._L(L), spec.encode(), _d(_cplx(U)), _d(_cplx(phi)), kappa, lam)
+
+    def wilson_loop(self, D, N, L, spec, U, Ra, Rb):
+        """spec "fund0": wilson_loop_fund; otherwise wilson_loop_rep in that irrep."""
+        return self.lib.ref_wilson_loop(D, N, self._L(L), spec.encode(), _d(_cplx(U)), Ra, Rb)
+
+    def polyakov_rep(self, D, N, L, spec, U, tdir):
+        return self.lib.ref_polyakov_rep(D, N, self._L(L), spec.encode(), _d(_cplx(U)), tdir)
 
     # multi-invariant onsite potential (src/action/scalar_invariants.hpp)
     def casimir_channels(self, N, spec):

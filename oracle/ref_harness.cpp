@@ -222,6 +222,21 @@ double ref_link_energy(int D, int N, const int* L, const char* spec, const doubl
 #undef CALL
 }
 
+// ---- loops traced in a probe irrep (src/measure/observables.hpp:36-101) ----
+double ref_wilson_loop(int D, int N, const int* L, const char* spec, const double* U, int Ra, int Rb) {
+#define CALL(DD, NN) { Lattice<DD> lat(ext<DD>(L)); GaugeField<DD, NN> G(lat); load_U(G, U); \
+    if (std::strcmp(spec, "fund0") == 0) return wilson_loop_fund<DD, NN>(G, Ra, Rb); \
+    auto* r = get_rep<NN>(spec); if (!r) return 0.0 / 0.0; return wilson_loop_rep<DD, NN>(G, *r, Ra, Rb); }
+  DISPATCH_DN(D, N, CALL)
+#undef CALL
+}
+double ref_polyakov_rep(int D, int N, const int* L, const char* spec, const double* U, int tdir) {
+#define CALL(DD, NN) { Lattice<DD> lat(ext<DD>(L)); GaugeField<DD, NN> G(lat); load_U(G, U); \
+    auto* r = get_rep<NN>(spec); if (!r) return 0.0 / 0.0; return polyakov_loop_rep<DD, NN>(G, *r, tdir); }
+  DISPATCH_DN(D, N, CALL)
+#undef CALL
+}
+
 // ---- multi-invariant onsite potential (src/action/scalar_invariants.hpp) ----
 // Channels: the distinct adjoint-Casimir eigenvalues of R (x) Rbar, in the
 // reference's order; returns their number (-1: bad N / spec).

@@ -194,11 +194,32 @@ def frozen_fixture():
     np.savez_compressed(os.path.join(HERE, "frozen_phi.npz"), **out)
 
 
-if __name__ == "__main__" and sys.argv[1:] == ["multi"]:
+def loops_fixture():
+    """Wilson loops (fundamental and in probe irreps) and Polyakov loops in probe irreps
+    of the reference (src/measure/observables.hpp:36-101) on hot configurations."""
+    out = {}
+    for name, D, N, L, sigma in [("su2_d4", 4, 2, [4, 3, 4, 5], 0.5), ("su3_d4", 4, 3, [3, 4, 2, 4], 0.4),
+                                 ("su3_d3", 3, 3, [4, 4, 3], 0.7)]:
+        U = R.hot_start(D, N, L, 7, sigma)
+        out[name + "_U"], out[name + "_L"] = U, np.array(L)
+        specs = ["fund0", "fund", "adj", "2", "3"] + (["2,1", "1,1", "3,1"] if N == 3 else ["4", "6"])
+        for spec in specs:
+            for Ra, Rb in [(1, 1), (2, 1), (2, 3)]:
+                out[f"{name}_W_{spec}_{Ra}x{Rb}"] = np.array(R.wilson_loop(D, N, L, spec, U, Ra, Rb))
+            if spec != "fund0":
+                for tdir in range(D):
+                    out[f"{name}_P_{spec}_{tdir}"] = np.array(R.polyakov_rep(D, N, L, spec, U, tdir))
+    np.savez_compressed(os.path.join(HERE, "loops.npz"), **out)
+
+
+if __name__ == "__main__" and sys.argv[1:] == ["loops"]:
+    loops_fixture()
+elif __name__ == "__main__" and sys.argv[1:] == ["multi"]:
     multi_fixture()
 elif __name__ == "__main__" and sys.argv[1:] == ["frozen"]:
     frozen_fixture()
 elif __name__ == "__main__":
+    loops_fixture()
     frozen_fixture()
     multi_fixture()
     rng_fixture()
