@@ -37,12 +37,13 @@ class Obs(C.Structure):
 
 class TrajRecord(C.Structure):
     _fields_ = [("dH", C.c_double), ("accepted", C.c_int), ("traj", C.c_int), ("plaquette", C.c_double),
-                ("L_phi", C.c_double), ("L_link", C.c_double), ("kappa", C.c_double)]
+                ("L_phi", C.c_double), ("L_link", C.c_double), ("kappa", C.c_double),
+                ("beta", C.c_double)]
 
 
 # numpy view of an array of TrajRecord
 TRAJ_DTYPE = [("dH", "f8"), ("accepted", "i4"), ("traj", "i4"), ("plaquette", "f8"), ("L_phi", "f8"),
-              ("L_link", "f8"), ("kappa", "f8")]
+              ("L_link", "f8"), ("kappa", "f8"), ("beta", "f8")]
 
 
 _dp = C.POINTER(C.c_double)
@@ -100,6 +101,7 @@ SIGNATURES = {
     "gh_set_potential_multi": [_ctx, C.c_int, _dp, C.c_double],
     "gh_set_potential_quartic": [_ctx],
     "gh_set_frozen_phi": [_ctx, C.c_int],
+    "gh_temper_interval": [_ctx, C.c_int],
     "gh_wilson_loop": [_ctx, C.c_int, C.c_int, C.c_int, _ip, C.c_int, _dp],
     "gh_polyakov_rep": [_ctx, C.c_int, C.c_int, _ip, C.c_int, _dp],
     "gh_normalize_phi": [_ctx],

@@ -45,6 +45,7 @@ struct gh_ctx {
   uint64_t bytes = 0;
   // tempering
   int temper = 0;
+  int temper_every = 1;
   uint64_t swap_seed = 0;
   int* t_order = nullptr;             // [nlat] lattice currently holding the k-th kappa (grouped)
   int* t_groups = nullptr;            // [ngroups+1] group boundaries into t_order
@@ -145,12 +146,17 @@ void enq_measure(gh_ctx* ctx, int slot) {
 }
 
 // Replica-tempering pass in kappa (src/hmc/replica_tempering.hpp:157-205 mechanism).
+// coupling 1: kappa (B = 2 V D L_link, the hopping term S_H = ... - kappa B);
+// coupling 2: beta  (B = P = n_plaq (plaquette - 1), S_g = -beta P + const,
+//                    src/hmc/replica_tempering.hpp:16-42).  Both: Delta = (c_i - c_j)(B_i - B_j).
 struct TemperArgs {
   LatDev* lats; const double* res; int* order; const int* groups; int ngroups; int D;
-  unsigned long long* stats; const int* pairmap; int nlat; unsigned long long seed;
+  unsigned long long* stats; const int* pairmap; int nlat; unsigned long long seed; int coupling;
+  int every;   // one swap pass after every `every` trajectories (ReplicaTempering::n_sweep)
 };
 __global__ void k_temper(const TemperArgs a) {
   if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  if (a.every > 1 && a.lats[0].traj % (unsigned long long)a.every != 0) return;
   unsigned long long& counter = a.stats[2 * a.nlat];
   for (int g = 0; g < a.ngroups; ++g) {
     const int b0 = a.groups[g], b1 = a.groups[g + 1];
@@ -161,16 +167,23 @@ __global__ void k_temper(const TemperArgs a) {
         LatDev& Lj = a.lats[lj];
         const double* ri = a.res + ((size_t)li * 2 + (Li.last_acc ? 1 : 0)) * NRES;
         const double* rj = a.res + ((size_t)lj * 2 + (Lj.last_acc ? 1 : 0)) * NRES;
-        const double Bi = 2.0 * ri[6] * (double)Li.V * a.D;
-        const double Bj = 2.0 * rj[6] * (double)Lj.V * a.D;
-        const double delta = (Li.kappa - Lj.kappa) * (Bi - Bj);
+        const bool beta = a.coupling == 2;
+        const double nplaq_i = (double)Li.V * (a.D * (a.D - 1) / 2), nplaq_j = (double)Lj.V * (a.D * (a.D - 1) / 2);
+        const double Bi = beta ? nplaq_i * (ri[5] - 1.0) : 2.0 * ri[6] * (double)Li.V * a.D;
+        const double Bj = beta ? nplaq_j * (rj[5] - 1.0) : 2.0 * rj[6] * (double)Lj.V * a.D;
+        const double delta = beta ? (Li.beta - Lj.beta) * (Bi - Bj) : (Li.kappa - Lj.kappa) * (Bi - Bj);
         const int pid = a.pairmap[k];
         a.stats[pid] += 1;
         bool acc = (delta <= 0.0);
         counter += 1;
         if (!acc) acc = ghrng::uniform(a.seed, ghrng::key(0x57A9, counter)) < exp(-delta);
-        if (acc) {
+        if (acc && beta) {
+          const double tb = Li.beta; Li.beta = Lj.beta; Lj.beta = tb;
+        }
+        if (acc && !beta) {
           const double tk = Li.kappa; Li.kappa = Lj.kappa; Lj.kappa = tk;
+        }
+        if (acc) {
           const int tc = Li.cidx; Li.cidx = Lj.cidx; Lj.cidx = tc;
           a.order[k] = lj; a.order[k + 1] = li;
           a.stats[a.nlat + pid] += 1;
@@ -195,10 +208,10 @@ void enq_trajectory(gh_ctx* ctx) {
   m.lats = b.lats; m.res = b.res; m.hist = b.hist; m.hist_cap = b.hist_cap; m.nlat = ctx->nlat; m.pure = ctx->scalar ? 0 : 1;
   k_metropolis<<<(ctx->nlat + 63) / 64, 64, 0, ctx->st>>>(m);
   ctx->eng->restore(b);
-  if (ctx->temper && ctx->scalar) {
+  if (ctx->temper && (ctx->scalar || ctx->temper == 2)) {
     TemperArgs t;
     t.lats = b.lats; t.res = b.res; t.order = ctx->t_order; t.groups = ctx->t_groups; t.ngroups = ctx->t_ngroups;
-    t.D = ctx->D; t.stats = ctx->t_stats; t.pairmap = ctx->t_pairmap; t.nlat = ctx->nlat; t.seed = ctx->swap_seed;
+    t.D = ctx->D; t.stats = ctx->t_stats; t.pairmap = ctx->t_pairmap; t.nlat = ctx->nlat; t.seed = ctx->swap_seed; t.coupling = ctx->temper; t.every = ctx->temper_every;
     k_temper<<<1, 32, 0, ctx->st>>>(t);
   }
 }
@@ -1055,6 +1068,7 @@ int gh_run_trajectories(gh_ctx* ctx, int ntraj, gh_traj_record* records) {
           const TrajRec& r = h[(size_t)l * cap + (int)(tr % (unsigned long long)cap)];
           gh_traj_record& o = records[(size_t)(t0 + t) * ctx->nlat + l];
           o.dH = r.dH; o.accepted = r.accepted; o.traj = r.traj; o.plaquette = r.plaq; o.L_phi = r.L_phi; o.L_link = r.L_link; o.kappa = r.kappa;
+          o.beta = r.beta;
         }
     }
   }
@@ -1085,6 +1099,7 @@ int gh_read_records(gh_ctx* ctx, int ntraj, gh_traj_record* records) {
       const unsigned long long tr = L[l].traj - (unsigned long long)(ntraj - t);
       const TrajRec& r = h[(size_t)l * cap + (int)(tr % (unsigned long long)cap)];
       o.dH = r.dH; o.accepted = r.accepted; o.traj = r.traj; o.plaquette = r.plaq; o.L_phi = r.L_phi; o.L_link = r.L_link; o.kappa = r.kappa;
+          o.beta = r.beta;
     }
   return GH_OK;
 }
@@ -1107,6 +1122,7 @@ int gh_trajectory_host(gh_ctx* ctx, double* U, double* phi, gh_traj_record* rec)
     CK(cudaMemcpy(&r, ctx->b.hist + slot, sizeof(r), cudaMemcpyDeviceToHost));
     rec->dH = r.dH; rec->accepted = r.accepted; rec->traj = r.traj; rec->plaquette = r.plaq; rec->L_phi = r.L_phi; rec->L_link = r.L_link;
     rec->kappa = r.kappa;
+    rec->beta = r.beta;
   } else {
     CK(cudaStreamSynchronize(ctx->st));
   }
@@ -1117,7 +1133,8 @@ int gh_temper_enable(gh_ctx* ctx, int mode, uint64_t swap_seed) {
   if (!ctx) return fail(nullptr, GH_ERR_ARG, "null context");
   invalidate_graph(ctx);
   if (mode == 0) { ctx->temper = 0; return GH_OK; }
-  if (!ctx->scalar) return fail(ctx, GH_ERR_STATE, "kappa tempering needs a scalar field");
+  if (mode != 1 && mode != 2) return fail(ctx, GH_ERR_ARG, "tempering mode: 1 (kappa) or 2 (beta)");
+  if (mode == 1 && !ctx->scalar) return fail(ctx, GH_ERR_STATE, "kappa tempering needs a scalar field");
   CK(cudaStreamSynchronize(ctx->st));
   std::vector<LatDev> L(ctx->nlat);
   CK(cudaMemcpy(L.data(), ctx->b.lats, sizeof(LatDev) * ctx->nlat, cudaMemcpyDeviceToHost));
@@ -1127,9 +1144,11 @@ int gh_temper_enable(gh_ctx* ctx, int mode, uint64_t swap_seed) {
   std::vector<int> order, gb(1, 0), pairmap;
   for (auto& kv : groups) {
     auto v = kv.second;
-    std::sort(v.begin(), v.end(), [&](int a, int b) { return L[a].kappa < L[b].kappa; });
+    auto cpl = [&](int l) { return mode == 2 ? L[l].beta : L[l].kappa; };
+    std::sort(v.begin(), v.end(), [&](int a, int b) { return cpl(a) < cpl(b); });
     for (size_t k = 0; k + 1 < v.size(); ++k)
-      if (!(L[v[k + 1]].kappa > L[v[k]].kappa)) return fail(ctx, GH_ERR_ARG, "kappa ladder of equal-extent lattices must be strictly increasing");
+      if (!(cpl(v[k + 1]) > cpl(v[k])))
+        return fail(ctx, GH_ERR_ARG, "the tempered coupling of equal-extent lattices must be strictly increasing");
     order.insert(order.end(), v.begin(), v.end());
     gb.push_back((int)order.size());
   }
@@ -1151,6 +1170,15 @@ int gh_temper_enable(gh_ctx* ctx, int mode, uint64_t swap_seed) {
   ctx->t_ngroups = (int)gb.size() - 1;
   ctx->temper = mode;
   ctx->swap_seed = swap_seed;
+  return GH_OK;
+}
+
+int gh_temper_interval(gh_ctx* ctx, int n_sweep) {
+  if (!ctx) return fail(nullptr, GH_ERR_ARG, "null context");
+  if (n_sweep < 1) return fail(ctx, GH_ERR_ARG, "n_sweep must be >= 1");
+  CK(cudaStreamSynchronize(ctx->st));
+  ctx->temper_every = n_sweep;
+  invalidate_graph(ctx);
   return GH_OK;
 }
 

@@ -914,7 +914,7 @@ static __global__ void k_finalize(const FinArgs a) {
 // uniform(key(0xE5 | 0xB2, traj)); NaN/Inf dH rejects (as in the reference,
 // where every comparison with NaN is false) and is counted.  Appends a record.
 // ---------------------------------------------------------------------------
-struct TrajRec { double dH; int accepted; int traj; double plaq, L_phi, L_link, kappa; };
+struct TrajRec { double dH; int accepted; int traj; double plaq, L_phi, L_link, kappa, beta; };
 struct MetroArgs { LatDev* lats; const double* res; TrajRec* hist; int hist_cap; int nlat; int pure; };
 static __global__ void k_metropolis(const MetroArgs a) {
   const int l = blockIdx.x * blockDim.x + threadIdx.x;
@@ -940,6 +940,7 @@ static __global__ void k_metropolis(const MetroArgs a) {
     h.L_phi = ro[7];
     h.L_link = ro[6];
     h.kappa = L.kappa;
+    h.beta = L.beta;
   }
 }
 

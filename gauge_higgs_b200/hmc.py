@@ -469,8 +469,15 @@ class Ensemble:
         self.ctx("gh_use_graph", int(bool(on)))
 
     # ---- tempering ----
-    def enable_tempering(self, on=True, swap_seed=0x5A7AB1EC):
-        self.ctx("gh_temper_enable", 1 if on else 0, int(swap_seed))
+    def enable_tempering(self, on=True, swap_seed=0x5A7AB1EC, coupling="kappa"):
+        """Replica tempering across equal-extent lattices (src/hmc/replica_tempering.hpp):
+        coupling "beta" (the reference's) or "kappa"."""
+        mode = {"kappa": 1, "beta": 2}[coupling] if on else 0
+        self.ctx("gh_temper_enable", mode, int(swap_seed))
+
+    def set_temper_interval(self, n_sweep):
+        """One swap pass after every n_sweep trajectories (ReplicaTempering::n_sweep)."""
+        self.ctx("gh_temper_interval", int(n_sweep))
 
     def tempering_stats(self):
         att = np.zeros(max(self.n_lat - 1, 1), np.uint64)

@@ -70,14 +70,14 @@ typedef struct {
 } gh_obs;
 
 /* One trajectory of one lattice: dH, accept, and the driver's measurements
- * after accept/reject (src/hmc_higgs.cpp:80-87); kappa is the hopping parameter
- * the trajectory ran at (it moves between lattices under kappa tempering). */
+ * after accept/reject (src/hmc_higgs.cpp:80-87); kappa and beta are the couplings
+ * the trajectory ran at (they move between lattices under tempering). */
 typedef struct {
   double dH;
   int accepted;
   int traj;
   double plaquette, L_phi, L_link;
-  double kappa;
+  double kappa, beta;
 } gh_traj_record;
 
 typedef struct gh_ctx gh_ctx;
@@ -194,17 +194,24 @@ int gh_get_tile(gh_ctx* ctx, int lat, int* tile);
 /* Use (1, default) or bypass (0) the captured trajectory graph. */
 int gh_use_graph(gh_ctx* ctx, int enable);
 
-/* ---- replica tempering in kappa across the lattices of a batch ----
- * The mechanism of ReplicaTempering::step / attempt_swap (src/hmc/replica_tempering.hpp:157-205)
- * with kappa as the tempered coupling: after every trajectory, adjacent-kappa
- * pairs of lattices with equal extents propose a configuration exchange with
- * Delta = (kappa_i - kappa_j)(B_i - B_j), B = sum_{x,mu} 2 Re phi_x^dag D(U) phi_{x+mu},
- * coin uniform(key(0x57A9, ++counter)) on swap_seed; even pass then odd pass.
+/* ---- replica tempering across the lattices of a batch ----
+ * ReplicaTempering::step / attempt_swap (src/hmc/replica_tempering.hpp:157-205):
+ * after every trajectory, adjacent pairs of the coupling ladder among lattices
+ * with equal extents propose a configuration exchange with
+ * Delta = (c_i - c_j)(B_i - B_j), coin uniform(key(0x57A9, ++counter)) on
+ * swap_seed; even pass then odd pass.
+ *   mode 2: beta, B = n_plaq (plaquette - 1)  -- the reference's tempering;
+ *   mode 1: kappa, B = sum_{x,mu} 2 Re phi_x^dag D(U) phi_{x+mu} (no counterpart
+ *           in the reference; same mechanism with kappa tempered);
+ *   mode 0: off.
  * The exchange swaps the coupling labels on the device (equivalent to swapping
- * U and phi).  mode 0 disables. */
+ * U and phi); the couplings each trajectory ran at are in its record. */
 int gh_temper_enable(gh_ctx* ctx, int mode, uint64_t swap_seed);
+/* One swap pass after every n_sweep trajectories (ReplicaTempering::n_sweep,
+ * src/hmc/replica_tempering.hpp:157-167; default 1). */
+int gh_temper_interval(gh_ctx* ctx, int n_sweep);
 /* attempts/accepts: per adjacent pair in ladder order (n_lat - 1 entries);
- * kappa_of_lat: current kappa of each lattice. */
+ * kappa_of_lat: current kappa of each lattice (see gh_get_couplings for beta). */
 int gh_temper_stats(gh_ctx* ctx, uint64_t* attempts, uint64_t* accepts, double* kappa_of_lat);
 
 /* ---- coupling-scan surrogate: an ensemble of MLPs trained on the GPU ----

@@ -13,11 +13,15 @@
 //   observables              avg_plaquette, higgs_length, link_energy, polyakov_loop
 //   Stats                    src/measure/observables.hpp:104-145
 //   CasimirChannels, MultiInvariantPotential   src/action/scalar_invariants.hpp:19-206
+//   ReplicaTempering<D,N>    src/hmc/replica_tempering.hpp (parallel tempering in beta)
 // Fields live on the GPU; U()/phi() copy them to host vectors in the reference's
 // layouts.  Errors throw std::runtime_error, as the reference does.
 #pragma once
+#include <algorithm>
 #include <array>
+#include <cctype>
 #include <cmath>
+#include <cstdlib>
 #include <cstdint>
 #include <sstream>
 #include <stdexcept>
@@ -274,6 +278,147 @@ class GaugeHMC : public GaugeHiggsHMC<D, N> {
  public:
   GaugeHMC(const std::array<int, D>& extents, std::uint64_t seed, Precision prec = Precision::FP64)
       : GaugeHiggsHMC<D, N>(extents, Representation{}, seed, prec) {}
+};
+
+// ---- parallel tempering in beta (src/hmc/replica_tempering.hpp) ----
+// Same interface as the reference's ReplicaTempering<D,N>: rung k holds beta_k; one
+// step() runs n_sweep trajectories of every rung, then (if enabled) the even and odd
+// swap passes.  All rungs live in one context and advance in the same launches; a
+// swap exchanges the beta labels on the device, which is the reference's exchange of
+// (U, phi) between rungs (each rung keeps its beta, the configurations migrate).
+template <int D, int N>
+class ReplicaTempering {
+ public:
+  std::vector<double> betas;
+  bool enabled = true;
+  int n_sweep = 1;
+
+  ReplicaTempering(const std::array<int, D>& extents, const Representation& R, const std::vector<double>& beta_ladder,
+                   std::uint64_t seed0, std::uint64_t seed_stride = 1000003ull, std::uint64_t swap_seed = 0x5A7AB1ECull,
+                   Precision prec = Precision::FP64)
+      : betas(beta_ladder), rep_(R), swap_seed_(swap_seed) {
+    if (beta_ladder.size() < 2) throw std::runtime_error("ReplicaTempering: need >=2 replicas");
+    for (size_t k = 1; k < beta_ladder.size(); ++k)
+      if (!(beta_ladder[k] > beta_ladder[k - 1])) throw std::runtime_error("ReplicaTempering: beta-ladder must be strictly increasing");
+    const int M = (int)beta_ladder.size();
+    std::vector<int> L;
+    std::vector<std::uint64_t> seeds;
+    for (int k = 0; k < M; ++k) {
+      L.insert(L.end(), extents.begin(), extents.end());
+      seeds.push_back(seed0 + (std::uint64_t)k * seed_stride);
+    }
+    gh_rep_desc desc = rep_.desc();
+    check(gh_ctx_create(D, N, M, L.data(), rep_.kind == GH_REP_NONE ? nullptr : &desc, (int)prec, seeds.data(), &ctx_), nullptr);
+    for (int k = 0; k < M; ++k) check(gh_set_couplings(ctx_, k, beta_ladder[k], kappa_, lambda_), ctx_);
+    rung_traj_.assign((size_t)M, 0);
+    rung_acc_.assign((size_t)M, 0);
+  }
+  ReplicaTempering(const ReplicaTempering&) = delete;
+  ReplicaTempering& operator=(const ReplicaTempering&) = delete;
+  ~ReplicaTempering() { gh_ctx_destroy(ctx_); }
+
+  std::size_t n_replicas() const { return betas.size(); }
+  std::size_t n_pairs() const { return betas.size() - 1; }
+  double beta(std::size_t k) const { return betas.at(k); }
+  gh_ctx* context() { return ctx_; }
+
+  void set_kappa(double kappa) { kappa_ = kappa; push_couplings(); }
+  void set_lambda(double lambda) { lambda_ = lambda; push_couplings(); }
+  void set_tau(double tau) { tau_ = tau; push_integrator(); }
+  void set_nmd(int nmd) { nmd_ = nmd; push_integrator(); }
+  void set_integrator(Integrator integ) { integ_ = integ; push_integrator(); }
+  void set_potential(const MultiInvariantPotential<N>* pot) {
+    if (pot) check(gh_set_potential_multi(ctx_, (int)pot->f.size(), pot->f.data(), pot->mu2), ctx_);
+    else check(gh_set_potential_quartic(ctx_), ctx_);
+  }
+  void set_frozen_phi(bool f) {
+    check(gh_set_frozen_phi(ctx_, f ? 1 : 0), ctx_);
+    if (f) check(gh_normalize_phi(ctx_), ctx_);
+  }
+  // start configurations of every rung (each with its own seed)
+  void hot(double sigma = 1.0) { check(gh_hot_start(ctx_, sigma), ctx_); }
+  void phi_gaussian(std::uint64_t stream, double sigma = 1.0) { check(gh_phi_gaussian(ctx_, stream, sigma), ctx_); }
+
+  // one cycle: n_sweep trajectories of every rung, then the swap passes (if enabled)
+  std::vector<gh_traj_record> step() {
+    if (enabled != pen_ || n_sweep != psw_) {
+      check(gh_temper_enable(ctx_, enabled ? 2 : 0, swap_seed_), ctx_);
+      check(gh_temper_interval(ctx_, n_sweep), ctx_);
+      pen_ = enabled; psw_ = n_sweep;
+    }
+    std::vector<gh_traj_record> r((size_t)n_sweep * n_replicas());
+    check(gh_run_trajectories(ctx_, n_sweep, r.data()), ctx_);
+    for (const gh_traj_record& x : r) {
+      const size_t k = rung_of(x.beta);
+      ++rung_traj_[k];
+      rung_acc_[k] += x.accepted ? 1 : 0;
+    }
+    return r;
+  }
+
+  std::uint64_t swap_attempts(std::size_t p) const { return stats().first.at(p); }
+  std::uint64_t swap_accepts(std::size_t p) const { return stats().second.at(p); }
+  double pair_acceptance(std::size_t p) const {
+    const auto st = stats();
+    return st.first.at(p) ? double(st.second.at(p)) / double(st.first.at(p)) : 0.0;
+  }
+  // HMC acceptance of the trajectories run at rung k's beta
+  double hmc_acceptance(std::size_t k) const {
+    return rung_traj_.at(k) ? double(rung_acc_.at(k)) / double(rung_traj_.at(k)) : 0.0;
+  }
+  // measurements of the configuration currently at rung k
+  gh_obs measure(std::size_t k) {
+    gh_obs o;
+    check(gh_measure(ctx_, lattice_at(k), &o), ctx_);
+    return o;
+  }
+  // GH_TEMPER: true unless unset or one of 0 / false / off / no (any case)
+  static bool env_enabled() {
+    const char* e = std::getenv("GH_TEMPER");
+    if (!e) return false;
+    std::string v(e);
+    for (auto& c : v) c = (char)std::tolower((unsigned char)c);
+    return !(v.empty() || v == "0" || v == "false" || v == "off" || v == "no");
+  }
+
+ private:
+  size_t rung_of(double b) const {
+    for (size_t k = 0; k < betas.size(); ++k)
+      if (betas[k] == b) return k;
+    throw std::runtime_error("ReplicaTempering: record with an unknown beta");
+  }
+  int lattice_at(std::size_t k) {
+    for (int l = 0; l < (int)betas.size(); ++l) {
+      double b, kp, lm;
+      check(gh_get_couplings(ctx_, l, &b, &kp, &lm), ctx_);
+      if (b == betas.at(k)) return l;
+    }
+    throw std::runtime_error("ReplicaTempering: rung not found");
+  }
+  void push_couplings() {
+    for (int l = 0; l < (int)betas.size(); ++l) {
+      double b, kp, lm;
+      check(gh_get_couplings(ctx_, l, &b, &kp, &lm), ctx_);
+      check(gh_set_couplings(ctx_, l, b, kappa_, lambda_), ctx_);
+    }
+  }
+  void push_integrator() {
+    check(gh_set_integrator(ctx_, integ_ == Integrator::Leapfrog ? GH_LEAPFROG : GH_OMELYAN, nmd_, tau_), ctx_);
+  }
+  std::pair<std::vector<std::uint64_t>, std::vector<std::uint64_t>> stats() const {
+    std::vector<std::uint64_t> a(betas.size()), c(betas.size());
+    check(gh_temper_stats(ctx_, a.data(), c.data(), nullptr), ctx_);
+    return {a, c};
+  }
+  Representation rep_;
+  std::uint64_t swap_seed_;
+  gh_ctx* ctx_ = nullptr;
+  double kappa_ = 0.1, lambda_ = 0.5, tau_ = 1.0;
+  int nmd_ = 20;
+  Integrator integ_ = Integrator::Omelyan2MN;
+  bool pen_ = false;
+  int psw_ = 0;
+  std::vector<std::uint64_t> rung_traj_, rung_acc_;
 };
 
 // ---- time-series statistics (src/measure/observables.hpp:104-145) ----

@@ -80,3 +80,43 @@ def test_hmc_higgs_multi_runs():
     r = subprocess.run([exe, "fund", "4", "2.3", "0.2", "1.0", "1,2,3"], capture_output=True, text=True, timeout=60)
     assert r.returncode == 1 and "need 2 couplings" in r.stderr
 
+
+
+CPP_TEMPER = r'''
+#include <cstdio>
+#include "gauge_higgs_b200.hpp"
+int main() {
+  ghb::ReplicaTempering<4, 2> pt({4, 4, 4, 4}, ghb::FundamentalRep<2>(), {2.2, 2.25, 2.3, 2.35}, 5);
+  pt.set_kappa(0.25); pt.set_lambda(0.5); pt.set_nmd(10);
+  pt.hot(0.8); pt.phi_gaussian(12345, 0.3);
+  for (int s = 0; s < 200; ++s) pt.step();
+  for (size_t p = 0; p < pt.n_pairs(); ++p)
+    std::printf("pair %zu attempts %llu accepts %llu\n", p, (unsigned long long)pt.swap_attempts(p), (unsigned long long)pt.swap_accepts(p));
+  for (size_t k = 0; k < pt.n_replicas(); ++k)
+    std::printf("rung %zu beta %.2f hmc_acc %.3f plaq %.6f\n", k, pt.beta(k), pt.hmc_acceptance(k), pt.measure(k).plaquette);
+  return 0;
+}
+'''
+
+
+def test_cpp_replica_tempering(tmp_path):
+    """ghb::ReplicaTempering (the reference's ReplicaTempering<D,N> interface) compiled
+    against include/ and the library: one swap pass per step, swaps accepted, every rung
+    accepts HMC trajectories, a plaquette measured at every rung."""
+    src = tmp_path / "pt.cpp"
+    src.write_text(CPP_TEMPER)
+    exe = tmp_path / "pt"
+    lib = os.path.join(ROOT, "gauge_higgs_b200", "lib")
+    r = subprocess.run(["g++", "-O2", "-std=c++17", "-I" + os.path.join(ROOT, "include"), str(src), "-o", str(exe),
+                        "-L" + lib, "-lgauge_higgs_b200", "-Wl,-rpath," + lib], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    r = subprocess.run([str(exe)], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr
+    pairs = [list(map(int, re.findall(r"attempts (\d+) accepts (\d+)", ln)[0])) for ln in r.stdout.splitlines()
+             if ln.startswith("pair")]
+    rungs = [re.findall(r"hmc_acc ([0-9.]+) plaq ([0-9.]+)", ln)[0] for ln in r.stdout.splitlines() if ln.startswith("rung")]
+    assert len(pairs) == 3 and all(a == 200 and 0 < c < a for a, c in (tuple(p) for p in pairs))
+    acc = [float(a) for a, _ in rungs]
+    plaq = [float(p) for _, p in rungs]
+    assert min(acc) > 0.5
+    assert all(0.4 < p < 0.8 for p in plaq)

@@ -354,6 +354,74 @@ def test_tempering_is_canonical():
     assert worst < 4.5, worst
 
 
+def _beta_ensemble(tempered, ntraj, seed0=11, n_sweep=1, higgs=True, precision="fp64"):
+    import gauge_higgs_b200 as gh
+    ext = [[4, 4, 4, 4]] * 4
+    betas = [2.2, 2.25, 2.3, 2.35]
+    rep = gh.FundamentalRep(2) if higgs else None
+    e = gh.Ensemble(ext, rep, seeds=[seed0 + 1000003 * i for i in range(4)], N=2, beta=betas, kappa=0.25, lam=0.5,
+                    nmd=10, precision=precision)
+    e.hot(0.8)
+    if higgs:
+        e.phi_gaussian(12345, 0.3)
+    if tempered:
+        e.enable_tempering(True, swap_seed=0x5A7AB1EC, coupling="beta")
+        e.set_temper_interval(n_sweep)
+    rec = e.run(ntraj)
+    e.close()
+    return betas, rec
+
+
+@pytest.mark.parametrize("n_sweep,higgs", [(1, True), (2, False)])
+def test_beta_tempering_replayed_on_host(n_sweep, higgs):
+    """The reference's tempering (src/hmc/replica_tempering.hpp:157-205): beta ladder,
+    Delta = (beta_i - beta_j)(P_i - P_j), P = n_plaq (plaquette - 1), one even + odd
+    pass after every n_sweep trajectories, coin uniform(key(0x57A9, ++counter)) --
+    every decision replayed on the host from the trajectory records."""
+    import math
+    from gauge_higgs_b200._lib import LIB
+    betas, rec = _beta_ensemble(True, 300, n_sweep=n_sweep, higgs=higgs)
+    nplaq, seed = 4 ** 4 * 6, 0x5A7AB1EC
+    b = np.array(betas)
+    assert np.array_equal(rec[0]["beta"], b)
+    attempt = nswaps = 0
+    for t in range(len(rec) - 1):
+        if (t + 1) % n_sweep == 0:
+            P = nplaq * (rec[t]["plaquette"] - 1.0)
+            order = list(np.argsort(b, kind="stable"))
+            for start in (0, 1):
+                for k in range(start, 3, 2):
+                    li, lj = order[k], order[k + 1]
+                    delta = (b[li] - b[lj]) * (P[li] - P[lj])
+                    attempt += 1
+                    if delta <= 0.0 or LIB.gh_rng_uniform(seed, LIB.gh_rng_key(0x57A9, attempt, 0, 0, 0)) < math.exp(-delta):
+                        b[li], b[lj] = b[lj], b[li]
+                        order[k], order[k + 1] = lj, li
+                        nswaps += 1
+        assert np.array_equal(rec[t + 1]["beta"], b), t
+    assert 0 < nswaps < attempt
+
+
+def test_beta_tempering_is_canonical():
+    """Per-beta <plaquette> and <L_link> of the tempered ensemble equal those of
+    independent fixed-beta chains (binned errors, 4.5 sigma) -- the property that
+    test/test_replica_tempering_canonical.cpp checks for the reference."""
+    from gauge_higgs_b200.stats import Stats
+    n, nth = 5000, 300
+    betas, rt = _beta_ensemble(True, n + nth, seed0=21)
+    _, ru = _beta_ensemble(False, n + nth, seed0=71)
+    rt, ru = rt[nth:], ru[nth:]
+    worst = 0.0
+    for i, bv in enumerate(betas):
+        for obs in ("plaquette", "L_link"):
+            xt = rt[obs][rt["beta"] == bv]
+            xu = ru[obs][:, i]
+            assert len(xt) == n
+            st, su = Stats(xt.astype(float)), Stats(xu.astype(float))
+            worst = max(worst, abs(st.mean() - su.mean()) / np.hypot(st.binned_error(), su.binned_error()))
+    assert worst < 4.5, worst
+
+
 # ---------------------------------------------------------------------------
 # kick tiles: results are independent of the block shape; the autotuner picks one
 # ---------------------------------------------------------------------------
