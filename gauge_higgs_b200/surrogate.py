@@ -4,7 +4,7 @@ Batched HMC (one Ensemble of independent lattices, one per coupling point)
 measures <L_link>, chi_link = V Var(L_link) and the plaquette; an MLP ensemble
 (gauge_higgs_b200.mlp, trained on the GPU) maps (beta, kappa, lambda, 1/L) to
 (<L_link>, log chi_link, plaquette); new points go where the ensemble is least
-certain about the transition.  Plain HMC at every chosen point is the judge.
+certain about the transition.  Plain HMC at every chosen point supplies the data.
 
 The estimator uses that S_H contains -kappa B with B = 2 V D L_link, so
 d<L_link>/dkappa = 2 D chi_link: the chi_link peak (the reference's transition

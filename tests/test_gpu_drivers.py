@@ -60,14 +60,13 @@ def test_driver_rejects_bad_rep():
     assert r.returncode == 1 and "rep error" in r.stderr
 
 
-def test_hmc_higgs_multi_runs():
+def test_hmc_higgs_multi_runs(tmp_path):
     """The multi-invariant potential driver (src/hmc_higgs_multi.cpp): channel listing,
     a short run with explicit couplings, its output lines and the time-series file."""
     exe = os.path.join(BIN, "hmc_higgs_multi")
     r = subprocess.run([exe, "fund"], capture_output=True, text=True, timeout=60)
     assert r.returncode == 0 and "2 quartic channels" in r.stdout
-    ts = os.path.join(ROOT, "gpurun_out", "multi_ts.txt") if os.path.isdir(os.path.join(ROOT, "gpurun_out")) else \
-        os.path.join("/tmp", "multi_ts.txt")
+    ts = str(tmp_path / "multi_ts.txt")
     r = subprocess.run([exe, "fund", "4", "2.3", "0.2", "1.0", "0.8,0.5", "20", "60", "16", "1.0", "3", ts],
                        capture_output=True, text=True, timeout=300)
     assert r.returncode == 0, r.stderr
