@@ -142,7 +142,7 @@ void enq_measure(gh_ctx* ctx, int slot) {
   FinArgs f;
   f.lats = ctx->b.lats; f.blk_first = ctx->b.blk_first; f.partials = ctx->b.partials; f.res = ctx->b.res;
   f.slot = slot; f.D = ctx->D; f.N = ctx->N; f.scalar = ctx->scalar;
-  k_finalize<<<ctx->nlat, 32, 0, ctx->st>>>(f);
+  launch(k_finalize, ctx->nlat, 32, 0, ctx->st, f);
 }
 
 // Replica-tempering pass in kappa (src/hmc/replica_tempering.hpp:157-205 mechanism).
@@ -155,6 +155,7 @@ struct TemperArgs {
   int every;   // one swap pass after every `every` trajectories (ReplicaTempering::n_sweep)
 };
 __global__ void k_temper(const TemperArgs a) {
+  pdl_enter();
   if (threadIdx.x != 0 || blockIdx.x != 0) return;
   if (a.every > 1 && a.lats[0].traj % (unsigned long long)a.every != 0) return;
   unsigned long long& counter = a.stats[2 * a.nlat];
@@ -206,13 +207,13 @@ void enq_trajectory(gh_ctx* ctx) {
   enq_measure(ctx, 1);
   MetroArgs m;
   m.lats = b.lats; m.res = b.res; m.hist = b.hist; m.hist_cap = b.hist_cap; m.nlat = ctx->nlat; m.pure = ctx->scalar ? 0 : 1;
-  k_metropolis<<<(ctx->nlat + 63) / 64, 64, 0, ctx->st>>>(m);
+  launch(k_metropolis, (ctx->nlat + 63) / 64, 64, 0, ctx->st, m);
   ctx->eng->restore(b);
   if (ctx->temper && (ctx->scalar || ctx->temper == 2)) {
     TemperArgs t;
     t.lats = b.lats; t.res = b.res; t.order = ctx->t_order; t.groups = ctx->t_groups; t.ngroups = ctx->t_ngroups;
     t.D = ctx->D; t.stats = ctx->t_stats; t.pairmap = ctx->t_pairmap; t.nlat = ctx->nlat; t.seed = ctx->swap_seed; t.coupling = ctx->temper; t.every = ctx->temper_every;
-    k_temper<<<1, 32, 0, ctx->st>>>(t);
+    launch(k_temper, 1, 32, 0, ctx->st, t);
   }
 }
 

@@ -6,6 +6,24 @@
 
 namespace ghk {
 
+// Launch with programmatic stream serialisation (see pdl_enter): the kernel may be
+// scheduled while the previous kernel in the stream drains.
+template <typename A>
+inline void launch(void (*kernel)(A), unsigned grid, unsigned block, size_t smem, cudaStream_t st, const A& args) {
+  if (grid == 0) return;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(grid);
+  cfg.blockDim = dim3(block);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = st;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  cudaLaunchKernelEx(&cfg, kernel, args);
+}
+
 struct Bufs {
   void *U, *Us, *P, *phi, *phis, *pi, *psif, *psib;
   LatDev* lats;
@@ -71,7 +89,7 @@ struct Engine : EngineBase {
     const int count = (links ? b.nwk_links : 0) + (do_sites ? b.nwk_sites : 0);
     if (count == 0) return;
     a.work = b.w_kick + first;
-    k_kick<D, N, R, REP><<<count, KICK_BLOCK, 0, b.st>>>(a);
+    launch(k_kick<D, N, R, REP>, count, KICK_BLOCK, 0, b.st, a);
   }
   void gen_links(const Bufs& b, double eps, int mode, double* out) override {
     if (REP != REP_GEN) return;
@@ -79,24 +97,24 @@ struct Engine : EngineBase {
     a.work = b.w_gen; a.lats = b.lats; a.U = b.U; a.P = b.P; a.phi = b.phi; a.psif = b.psif; a.psib = b.psib;
     a.t = b.gen; a.eps = eps; a.mode = mode; a.out = out;
     const size_t sm = gen_smem(b);
-    k_gen_links<D, N, R><<<b.nw_gen, b.gen_warps * 32, sm, b.st>>>(a);
+    launch(k_gen_links<D, N, R>, b.nw_gen, b.gen_warps * 32, sm, b.st, a);
   }
   void drift(const Bufs& b, double eps, int reunit) override {
     DriftArgs a;
     a.work = b.w_all; a.lats = b.lats; a.U = b.U; a.P = b.P; a.phi = b.phi; a.pi = b.pi;
     a.eps = eps; a.reunit = reunit; a.d = b.d; a.frozen = b.frozen;
-    k_drift<N, R><<<b.nw_links + (b.scalar ? b.nw_sites : 0), KBLOCK, 0, b.st>>>(a);
+    launch(k_drift<N, R>, b.nw_links + (b.scalar ? b.nw_sites : 0), KBLOCK, 0, b.st, a);
   }
   void sphere(const Bufs& b, int what) override {
     if (!b.scalar) return;
     SphereArgs a;
     a.work = b.w_all + b.nw_links; a.lats = b.lats; a.phi = b.phi; a.pi = b.pi; a.d = b.d; a.what = what;
-    k_sphere<R><<<b.nw_sites, KBLOCK, 0, b.st>>>(a);
+    launch(k_sphere<R>, b.nw_sites, KBLOCK, 0, b.st, a);
   }
   void reunit(const Bufs& b) override {
     LinkArgs a;
     a.work = b.w_all; a.lats = b.lats; a.U = b.U; a.Us = b.Us;
-    k_reunit<N, R><<<b.nw_links, KBLOCK, 0, b.st>>>(a);
+    launch(k_reunit<N, R>, b.nw_links, KBLOCK, 0, b.st, a);
   }
   void measure(const Bufs& b) override {
     if (REP == REP_GEN && b.scalar) gen_links(b, 0.0, 1, nullptr);
@@ -104,7 +122,7 @@ struct Engine : EngineBase {
     a.work = b.w_all + b.nw_links; a.lats = b.lats; a.U = b.U; a.P = b.P; a.phi = b.phi; a.pi = b.pi;
     a.psif = b.psif; a.d = b.d; a.scalar = b.scalar; a.partials = b.partials;
     a.pot = b.pot; a.mu2 = b.mu2; a.asup = b.asup64;
-    k_measure<D, N, R, REP><<<b.nw_sites, KBLOCK, 0, b.st>>>(a);
+    launch(k_measure<D, N, R, REP>, b.nw_sites, KBLOCK, 0, b.st, a);
   }
   void init(const Bufs& b, InitArgs a, bool links, bool sites) override {
     a.lats = b.lats; a.U = b.U; a.P = b.P;
@@ -112,12 +130,12 @@ struct Engine : EngineBase {
     const int count = (links ? b.nw_links : 0) + (sites ? b.nw_sites : 0);
     if (count == 0) return;
     a.work = b.w_all + first;
-    k_init<N, R><<<count, KBLOCK, 0, b.st>>>(a);
+    launch(k_init<N, R>, count, KBLOCK, 0, b.st, a);
   }
   void restore(const Bufs& b) override {
     RestoreArgs a;
     a.work = b.w_all; a.lats = b.lats; a.U = b.U; a.Us = b.Us; a.phi = b.phi; a.phis = b.phis; a.N = N; a.d = b.d;
-    k_restore<R><<<b.nw_links + (b.scalar ? b.nw_sites : 0), KBLOCK, 0, b.st>>>(a);
+    launch(k_restore<R>, b.nw_links + (b.scalar ? b.nw_sites : 0), KBLOCK, 0, b.st, a);
   }
   void polyakov(const Bufs& b, int tdir) override {
     PolyArgs a;

@@ -38,6 +38,16 @@ constexpr int ULANE = 32;      // sites per block of the link-field layout
 enum { POT_QUARTIC = 0, POT_MULTI = 1 };
 constexpr int POT_DMAX = 32;   // largest representation the multi-invariant potential accepts
 
+// Programmatic dependent launch: kernels of the MD path are launched so that the
+// next one in the stream may be scheduled while this one finishes.  Each waits for
+// its predecessor's results (griddepcontrol.wait: the predecessor grid has completed
+// and its writes are visible) before reading anything, then lets its own successor
+// launch.  Without the launch attribute both instructions are no-ops.
+__device__ __forceinline__ void pdl_enter() {
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
 struct LatDev {
   int L[4];
   int stride[4];
@@ -432,6 +442,7 @@ template <> struct KickMinBlocks<double> {
 
 template <int D, int N, typename R, int REP>
 __global__ void __launch_bounds__(KICK_BLOCK, KickMinBlocks<R>::v) k_kick(const KickArgs a) {
+  pdl_enter();
   const Work w = a.work[blockIdx.x];
   const LatDev& L = a.lats[w.lat];
   int s, x[D];
@@ -511,6 +522,7 @@ __device__ void gen_apply(const GenTables& t, const Mat<N, C>& M, bool dag, cons
 
 template <int D, int N, typename R>
 __global__ void __launch_bounds__(GEN_WARPS * 32) k_gen_links(const GenArgs a) {
+  pdl_enter();
   typedef typename Cmp<R>::t C;
   extern __shared__ unsigned char smem_raw[];
   const Work w = a.work[blockIdx.x];
@@ -629,6 +641,7 @@ struct DriftArgs {
 };
 template <int N, typename R>
 __global__ void __launch_bounds__(KBLOCK) k_drift(const DriftArgs a) {
+  pdl_enter();
   const Work w = a.work[blockIdx.x];
   if ((int)threadIdx.x >= w.n) return;
   const LatDev L = a.lats[w.lat];
@@ -699,6 +712,7 @@ __global__ void __launch_bounds__(KBLOCK) k_drift(const DriftArgs a) {
 struct SphereArgs { const Work* work; const LatDev* lats; void* phi; void* pi; int d; int what; };
 template <typename R>
 __global__ void __launch_bounds__(KBLOCK) k_sphere(const SphereArgs a) {
+  pdl_enter();
   const Work w = a.work[blockIdx.x];
   if ((int)threadIdx.x >= w.n) return;
   const LatDev& L = a.lats[w.lat];
@@ -732,6 +746,7 @@ __global__ void __launch_bounds__(KBLOCK) k_sphere(const SphereArgs a) {
 struct LinkArgs { const Work* work; const LatDev* lats; void* U; const void* Us; };
 template <int N, typename R>
 __global__ void __launch_bounds__(KBLOCK) k_reunit(const LinkArgs a) {
+  pdl_enter();
   const Work w = a.work[blockIdx.x];
   if ((int)threadIdx.x >= w.n || w.mu < 0) return;
   const LatDev L = a.lats[w.lat];
@@ -774,6 +789,7 @@ __device__ __forceinline__ double warp_sum(double v) {
 
 template <int D, int N, typename R, int REP>
 __global__ void __launch_bounds__(KBLOCK) k_measure(const MeasArgs a) {
+  pdl_enter();
   const Work w = a.work[blockIdx.x];
   double r[NRED] = {0, 0, 0, 0, 0, 0};
   if ((int)threadIdx.x < w.n) {
@@ -876,6 +892,7 @@ struct FinArgs {
   int scalar;
 };
 static __global__ void k_finalize(const FinArgs a) {
+  pdl_enter();
   const int l = blockIdx.x;
   const int b0 = a.blk_first[l], b1 = a.blk_first[l + 1];
   __shared__ double sh[NRED][32];
@@ -917,6 +934,7 @@ static __global__ void k_finalize(const FinArgs a) {
 struct TrajRec { double dH; int accepted; int traj; double plaq, L_phi, L_link, kappa, beta; };
 struct MetroArgs { LatDev* lats; const double* res; TrajRec* hist; int hist_cap; int nlat; int pure; };
 static __global__ void k_metropolis(const MetroArgs a) {
+  pdl_enter();
   const int l = blockIdx.x * blockDim.x + threadIdx.x;
   if (l >= a.nlat) return;
   LatDev& L = a.lats[l];
@@ -948,6 +966,7 @@ static __global__ void k_metropolis(const MetroArgs a) {
 struct RestoreArgs { const Work* work; const LatDev* lats; void* U; const void* Us; void* phi; const void* phis; int N; int d; };
 template <typename R>
 __global__ void __launch_bounds__(KBLOCK) k_restore(const RestoreArgs a) {
+  pdl_enter();
   const Work w = a.work[blockIdx.x];
   if ((int)threadIdx.x >= w.n) return;
   const LatDev& L = a.lats[w.lat];
@@ -997,6 +1016,7 @@ template <typename R> __device__ __forceinline__ double gauss_r(uint64_t seed, u
 
 template <int N, typename R>
 __global__ void __launch_bounds__(KBLOCK) k_init(const InitArgs a) {
+  pdl_enter();
   typedef typename Cmp<R>::t C;
   const Work w = a.work[blockIdx.x];
   if ((int)threadIdx.x >= w.n) return;
@@ -1049,6 +1069,7 @@ __global__ void __launch_bounds__(KBLOCK) k_init(const InitArgs a) {
 struct PolyArgs { const Work* work; const LatDev* lats; const void* U; int tdir; double* partials; };
 template <int D, int N, typename R>
 __global__ void __launch_bounds__(KBLOCK) k_polyakov(const PolyArgs a) {
+  pdl_enter();
   const Work w = a.work[blockIdx.x];
   double v = 0.0;
   if ((int)threadIdx.x < w.n) {
@@ -1144,6 +1165,7 @@ struct LoopArgs {
 };
 template <int D, int N, typename R>
 __global__ void __launch_bounds__(KBLOCK) k_loops(const LoopArgs a) {
+  pdl_enter();
   const Work w = a.work[blockIdx.x];
   double v = 0.0;
   if ((int)threadIdx.x < w.n) {
@@ -1211,6 +1233,7 @@ __global__ void __launch_bounds__(KBLOCK) k_loops(const LoopArgs a) {
 struct XferArgs { const LatDev* lats; int lat; int kind; int D; int ncomp; double* host_aos; void* dev; int to_dev; };
 template <typename R>
 __global__ void k_xfer(const XferArgs a) {
+  pdl_enter();
   const LatDev L = a.lats[a.lat];
   const long long per_site = (a.kind == 2) ? a.ncomp : (long long)a.D * a.ncomp;
   const long long total = (long long)L.V * per_site;
