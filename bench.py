@@ -453,6 +453,33 @@ def run_extra(a, dist):
                     "site_updates_per_s": round(v * sites * 20 * 2, 1), "acceptance": float(rec["accepted"].mean()),
                     "swap_acceptance": float(acc.sum() / max(att.sum(), 1)), "cpu_baseline": cpu})
         ens.close()
+    if wl in ("stage0", "all"):
+        # the reference's SU(2) -> 2I shakedown point (scripts/su2_stage0.sh: hmc_higgs_multi with
+        # rep {12}, d = 13, mu2 = 0.065 and its 13 channel couplings, beta = 2.0, nmd = 20, tau = 1)
+        f2i = [0.1182, 0.0819, 0.0353, 0.0274, 0.1550, 0.0828, 0.0157, 0.0702, 0.1083, 0.1143, 0.0189, 0.1124, 0.0595]
+        for Lx in (4, 8):
+            for prec in ("fp64", "fp32"):
+                rep = gh.GeneralRep(2, [12])
+                h = gh.GaugeHiggsHMC([Lx] * 4, rep, seed=1, precision=prec, beta=2.0, kappa=0.1, lam=0.5, nmd=20)
+                h.potential = gh.MultiInvariantPotential(gh.CasimirChannels(rep), f2i, 0.065)
+                h.hot(0.8)
+                h.phi_gaussian(12345, 0.3)
+                v, rec = gpu_rate(h, 40 if Lx == 4 else 10, W=2)
+                cpu = None
+                if prec == "fp64" and Lx == 4 and ref is not None:
+                    s = RefSession(ref, 4, 2, [Lx] * 4, "12", 2.0, 0.1, 0.5, 20, 1.0, 1, OMELYAN, 0.8, 0.3)
+                    s.set_multi(f2i, 0.065)
+                    s.run(1)
+                    t0 = time.perf_counter()
+                    s.run(3)
+                    cpu = {"value": round(3 / (time.perf_counter() - t0), 5), "cores": cores, "kind": "reference",
+                           "sample": "3 trajectories after one"}
+                    s.close()
+                out.append({"workload": f"SU(2) {{12}} (d=13) {Lx}^4, multi-invariant potential (13 channels, mu2=0.065), "
+                                        "beta=2.0 kappa=0.1, Omelyan nmd=20, hot start", "precision": prec,
+                            "value": round(v, 2), "unit": "trajectories/s",
+                            "acceptance": float(rec["accepted"].mean()), "cpu_baseline": cpu})
+                h.close()
     if wl in ("big", "all"):
         for prec in ("fp64", "fp32"):
             L = [32, 32, 32, 32]
@@ -524,7 +551,7 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--validate-traj", type=int, default=2000)
     ap.add_argument("--validate-therm", type=int, default=200)
-    ap.add_argument("--workload", default="c2", choices=["c2", "c1", "c3", "c4", "big", "validate", "all"],
+    ap.add_argument("--workload", default="c2", choices=["c2", "c1", "c3", "c4", "big", "stage0", "validate", "all"],
                     help="c2 (default) prints the headline line; the others print additional measurements")
     a = ap.parse_args()
     if a.warmup < 3 and a.impl == "ours":

@@ -96,6 +96,8 @@ SIGNATURES = {
     "gh_temper_stats": [_ctx, _u64p, _u64p, _dp],
     "gh_rep_general_info": [C.c_int, _ip, C.c_int, _ip, _ip, C.POINTER(C.c_long)],
     "gh_rep_general_build": [C.c_int, _ip, C.c_int, _dp, _dp],
+    "gh_rep_path": [_ctx, _ip],
+    "gh_sympow_matrix": [C.c_int, C.POINTER(RepDesc), _dp, _dp, C.POINTER(C.c_long)],
     "gh_casimir_channels": [C.c_int, C.POINTER(RepDesc), _dp, C.c_int, _ip],
     "gh_multi_superop": [C.c_int, C.POINTER(RepDesc), C.c_int, _dp, _dp],
     "gh_set_potential_multi": [_ctx, C.c_int, _dp, C.c_double],

@@ -12,6 +12,7 @@
 #include <vector>
 #include "gh_engine.cuh"
 #include "gh_potential.h"
+#include "gh_sympow.h"
 #include "../../include/gauge_higgs_b200.h"
 
 using namespace ghk;
@@ -57,15 +58,27 @@ struct gh_ctx {
   size_t wk_cap = 0;
   // general irreps: host copy of the generators T^a_R (multi-invariant potential set-up)
   std::vector<double> T_host;
-  // multi-invariant potential: device copies of the channel superoperator
-  double2* asup64 = nullptr;
-  float2* asup32 = nullptr;
-  size_t asup_cap = 0;
+  // general irreps: closed-form D(U) term lists (single-row irreps, when cheaper than
+  // the tensor path or when the tensor buffer does not fit in shared memory)
+  ghsym::Terms sp;
+  bool use_sp = false;
+  size_t gen_warp_bytes = 0;
+  // multi-invariant potential: device copies of the channel superoperator (sparse rows)
+  int* sa_ptr = nullptr;
+  unsigned short* sa_ij = nullptr;
+  double2* sa_v64 = nullptr;
+  float2* sa_v32 = nullptr;
+  void free_potential() {
+    if (sa_ptr) cudaFree(sa_ptr);
+    if (sa_ij) cudaFree(sa_ij);
+    if (sa_v64) cudaFree(sa_v64);
+    if (sa_v32) cudaFree(sa_v32);
+    sa_ptr = nullptr; sa_ij = nullptr; sa_v64 = nullptr; sa_v32 = nullptr;
+  }
   ~gh_ctx() {
     if (st) cudaStreamSynchronize(st);
     if (wk_dev) cudaFree(wk_dev);
-    if (asup64) cudaFree(asup64);
-    if (asup32) cudaFree(asup32);
+    free_potential();
     if (gexec) cudaGraphExecDestroy(gexec);
     if (graph) cudaGraphDestroy(graph);
     for (void* p : allocs) cudaFree(p);
@@ -364,7 +377,7 @@ int rebuild_kick_table(gh_ctx* ctx) {
 int build_general(gh_ctx* ctx, const gh_rep_desc* r) {
   const int d = r->d, N = ctx->N, ng = ctx->ng;
   const long dimT = r->dimT;
-  if (d <= 0 || r->n_boxes <= 0 || r->n_boxes > 15 || dimT <= 0 || !r->T || !r->W)
+  if (d <= 0 || r->n_boxes <= 0 || r->n_boxes > 17 || dimT <= 0 || !r->T || !r->W)
     return fail(ctx, GH_ERR_REP, "general representation needs d, n_boxes, dimT, T and W");
   long pw = 1;
   for (int k = 0; k < r->n_boxes; ++k) pw *= N;
@@ -400,7 +413,7 @@ int build_general(gh_ctx* ctx, const gh_rep_desc* r) {
   GenTables& t = ctx->b.gen;
   t.d = d; t.n = r->n_boxes; t.dimT = (int)dimT; t.ng = ng;
   t.powN[0] = 1;
-  for (int k = 1; k < 16; ++k) t.powN[k] = (k <= r->n_boxes) ? t.powN[k - 1] * N : 0;
+  for (int k = 1; k < 18; ++k) t.powN[k] = (k <= r->n_boxes) ? t.powN[k - 1] * N : 0;
   int *p1, *p2, *p3, *p4, *p5, *p6;
   double2 *v1, *v2, *v3;
   int rc;
@@ -418,6 +431,20 @@ int build_general(gh_ctx* ctx, const gh_rep_desc* r) {
   if (!t_j.empty()) CK(cudaMemcpy(p6, t_j.data(), t_j.size() * 4, cudaMemcpyHostToDevice));
   if (!t_v.empty()) CK(cudaMemcpy(v3, t_v.data(), t_v.size() * 16, cudaMemcpyHostToDevice));
   t.wt_ptr = p1; t.wt_l = p2; t.wt_v = v1; t.w_ptr = p3; t.w_i = p4; t.w_v = v2; t.t_ptr = p5; t.t_j = p6; t.t_v = v3;
+  t.sp_ptr = nullptr; t.sp_c = nullptr; t.sp_e = nullptr;
+  t.warp_bytes = (int)ctx->gen_warp_bytes;
+  if (ctx->use_sp) {
+    const ghsym::Terms& q = ctx->sp;
+    int* sptr;
+    double2* sc;
+    unsigned char* se;
+    if ((rc = dalloc(ctx, &sptr, q.ptr.size())) || (rc = dalloc(ctx, &sc, q.c.size() / 2)) || (rc = dalloc(ctx, &se, q.e.size())))
+      return rc;
+    CK(cudaMemcpy(sptr, q.ptr.data(), q.ptr.size() * 4, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(sc, q.c.data(), q.c.size() * 8, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(se, q.e.data(), q.e.size(), cudaMemcpyHostToDevice));
+    t.sp_ptr = sptr; t.sp_c = sc; t.sp_e = se;
+  }
   return GH_OK;
 }
 
@@ -429,6 +456,12 @@ int build_general(gh_ctx* ctx, const gh_rep_desc* r) {
 extern "C" {
 
 const char* gh_last_error(const gh_ctx* ctx) { return ctx ? ctx->err.c_str() : g_err.c_str(); }
+
+int gh_rep_path(const gh_ctx* ctx, int* path) {
+  if (!ctx || !path) return fail(nullptr, GH_ERR_ARG, "null argument");
+  *path = ctx->rep != REP_GEN ? GH_PATH_REGISTER : (ctx->use_sp ? GH_PATH_CLOSED_FORM : GH_PATH_TENSOR);
+  return GH_OK;
+}
 
 uint64_t gh_rng_key(uint64_t a, uint64_t b, uint64_t c, uint64_t d, uint64_t e) { return ghrng::key(a, b, c, d, e); }
 double gh_rng_uniform(uint64_t seed, uint64_t key) { return ghrng::uniform(seed, key); }
@@ -496,8 +529,25 @@ int gh_ctx_create(int D, int N, int n_lat, const int* L, const gh_rep_desc* rep,
   std::vector<Work> wg;
   int gw = GEN_WARPS;
   if (ctx->rep == REP_GEN) {
-    // one warp per link holds a tensor buffer of N^n complex numbers in shared memory
-    const size_t per_warp = ((size_t)rep->dimT + 4 * (size_t)rep->d) * 2 * ctx->rs;
+    // one warp per link.  Tensor path: a buffer of N^n complex numbers in shared memory.
+    // Single-row irreps: D(U) in closed form (d*d + N*N*(n+1) FP64 complex) when that
+    // costs fewer operations than the two slot sweeps of the tensor path, or when the
+    // tensor buffer does not fit.
+    const size_t cs = 2 * ctx->rs;
+    const size_t tensor_warp = ((size_t)rep->dimT + 4 * (size_t)rep->d) * cs;
+    if (rep->W && rep->d > 0 && rep->n_boxes >= 1 && rep->n_boxes <= 17 && rep->dimT > 0 && rep->dimT <= 200000) {
+      std::string why;
+      if (ghsym::build(N, rep->n_boxes, rep->d, rep->dimT, rep->W, 1L << 22, ctx->sp, &why)) {
+        const double term_ops = (double)(ctx->sp.c.size() / 2) * N * N + 2.0 * rep->d * rep->d;
+        const double tensor_ops = 2.0 * rep->n_boxes * (double)rep->dimT * N;
+        ctx->use_sp = term_ops < tensor_ops || tensor_warp > 227 * 1024;
+      }
+    }
+    size_t per_warp = ctx->use_sp
+        ? ((size_t)rep->d * rep->d + (size_t)N * N * (rep->n_boxes + 1)) * 16 + 4 * (size_t)rep->d * cs
+        : tensor_warp;
+    per_warp = (per_warp + 15) / 16 * 16;
+    ctx->gen_warp_bytes = per_warp;
     while (gw > 1 && gw * per_warp > 227 * 1024) gw /= 2;
     if (per_warp > 227 * 1024) return fail(nullptr, GH_ERR_REP, "general irrep too large for the shared-memory tensor buffer");
     for (int l = 0; l < n_lat; ++l)
@@ -996,24 +1046,40 @@ int gh_set_potential_multi(gh_ctx* ctx, int n_channels, const double* f, double 
   int rc = ghpot::superop(ctx->N, kind, ctx->d, ctx->T_host.empty() ? nullptr : ctx->T_host.data(),
                           std::vector<double>(f, f + n_channels), c2, A, err);
   if (rc) return fail(ctx, rc, err);
-  const size_t n = (size_t)ctx->d * ctx->d * ctx->d * ctx->d;
-  CK(cudaStreamSynchronize(ctx->st));
-  if (n > ctx->asup_cap) {
-    if (ctx->asup64) cudaFree(ctx->asup64);
-    if (ctx->asup32) cudaFree(ctx->asup32);
-    ctx->asup64 = nullptr;
-    ctx->asup32 = nullptr;
-    ctx->asup_cap = 0;
-    CK(cudaMalloc(&ctx->asup64, n * sizeof(double2)));
-    CK(cudaMalloc(&ctx->asup32, n * sizeof(float2)));
-    ctx->asup_cap = n;
+  // sparse rows: entries below 1e-15 of the largest are the rounding residue of the
+  // projector construction where A vanishes exactly (weight conservation)
+  const int d = ctx->d, dd = d * d;
+  double amax = 0.0;
+  for (size_t k = 0; k < (size_t)dd * dd; ++k) amax = std::max(amax, std::hypot(A[2 * k], A[2 * k + 1]));
+  std::vector<int> ptr(dd + 1, 0);
+  std::vector<unsigned short> ij;
+  std::vector<double2> v64;
+  std::vector<float2> v32;
+  for (int rq = 0; rq < dd; ++rq) {
+    for (int c = 0; c < dd; ++c) {
+      const size_t k = (size_t)rq * dd + c;
+      if (std::hypot(A[2 * k], A[2 * k + 1]) <= 1e-15 * amax) continue;
+      ij.push_back((unsigned short)((c / d) | ((c % d) << 8)));
+      v64.push_back(make_double2(A[2 * k], A[2 * k + 1]));
+      v32.push_back(make_float2((float)A[2 * k], (float)A[2 * k + 1]));
+    }
+    ptr[rq + 1] = (int)ij.size();
   }
-  std::vector<float2> a32(n);
-  for (size_t i = 0; i < n; ++i) a32[i] = make_float2((float)A[2 * i], (float)A[2 * i + 1]);
-  CK(cudaMemcpy(ctx->asup64, A.data(), n * sizeof(double2), cudaMemcpyHostToDevice));
-  CK(cudaMemcpy(ctx->asup32, a32.data(), n * sizeof(float2), cudaMemcpyHostToDevice));
-  ctx->b.asup64 = ctx->asup64;
-  ctx->b.asup32 = ctx->asup32;
+  const size_t nz = std::max<size_t>(ij.size(), 1);
+  CK(cudaStreamSynchronize(ctx->st));
+  ctx->free_potential();
+  CK(cudaMalloc(&ctx->sa_ptr, ptr.size() * sizeof(int)));
+  CK(cudaMalloc(&ctx->sa_ij, nz * sizeof(unsigned short)));
+  CK(cudaMalloc(&ctx->sa_v64, nz * sizeof(double2)));
+  CK(cudaMalloc(&ctx->sa_v32, nz * sizeof(float2)));
+  CK(cudaMemcpy(ctx->sa_ptr, ptr.data(), ptr.size() * sizeof(int), cudaMemcpyHostToDevice));
+  if (!ij.empty()) {
+    CK(cudaMemcpy(ctx->sa_ij, ij.data(), ij.size() * sizeof(unsigned short), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(ctx->sa_v64, v64.data(), v64.size() * sizeof(double2), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(ctx->sa_v32, v32.data(), v32.size() * sizeof(float2), cudaMemcpyHostToDevice));
+  }
+  ctx->b.sa64 = PotA{ctx->sa_ptr, ctx->sa_ij, ctx->sa_v64};
+  ctx->b.sa32 = PotA{ctx->sa_ptr, ctx->sa_ij, ctx->sa_v32};
   ctx->b.pot = POT_MULTI;
   ctx->b.mu2 = mu2;
   invalidate_graph(ctx);

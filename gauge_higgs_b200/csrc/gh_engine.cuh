@@ -44,8 +44,7 @@ struct Bufs {
   int frozen;            // frozen-length scalar |phi_x| = 1
   int pot;               // POT_QUARTIC or POT_MULTI
   double mu2;
-  const double2* asup64; // multi-invariant potential superoperator, FP64 and FP32 copies
-  const float2* asup32;
+  PotA sa64, sa32;       // multi-invariant potential superoperator, FP64 and FP32 values
   cudaStream_t st;
 };
 
@@ -71,7 +70,7 @@ struct Engine : EngineBase {
   typedef typename Cmp<R>::t C;
   Engine() {}
   size_t gen_smem(const Bufs& b) const override {
-    return (size_t)b.gen_warps * (b.gen.dimT + 4 * b.gen.d) * sizeof(cx<C>);
+    return (size_t)b.gen_warps * b.gen.warp_bytes;
   }
   int prepare(const Bufs& b) override {
     if (REP != REP_GEN) return 0;
@@ -83,7 +82,7 @@ struct Engine : EngineBase {
     a.lats = b.lats; a.U = b.U; a.P = b.P; a.phi = b.phi; a.pi = b.pi; a.psif = b.psif; a.psib = b.psib;
     a.eps = eps; a.mode = mode; a.flags = flags; a.d = b.d; a.out = out;
     a.pot = b.pot; a.mu2 = b.mu2;
-    a.asup = sizeof(R) == sizeof(double) ? (const void*)b.asup64 : (const void*)b.asup32;
+    a.sa = sizeof(R) == sizeof(double) ? b.sa64 : b.sa32;
     const bool do_sites = sites && b.scalar;
     const int first = links ? 0 : b.nwk_links;
     const int count = (links ? b.nwk_links : 0) + (do_sites ? b.nwk_sites : 0);
@@ -121,7 +120,7 @@ struct Engine : EngineBase {
     MeasArgs a;
     a.work = b.w_all + b.nw_links; a.lats = b.lats; a.U = b.U; a.P = b.P; a.phi = b.phi; a.pi = b.pi;
     a.psif = b.psif; a.d = b.d; a.scalar = b.scalar; a.partials = b.partials;
-    a.pot = b.pot; a.mu2 = b.mu2; a.asup = b.asup64;
+    a.pot = b.pot; a.mu2 = b.mu2; a.sa = b.sa64;
     launch(k_measure<D, N, R, REP>, b.nw_sites, KBLOCK, 0, b.st, a);
   }
   void init(const Bufs& b, InitArgs a, bool links, bool sites) override {

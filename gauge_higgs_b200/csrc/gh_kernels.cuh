@@ -36,6 +36,10 @@ constexpr int GEN_WARPS = 4;   // warps per block of the general-irrep kernel
 constexpr int NRED = 6;        // per-site partial sums of the measure kernel
 constexpr int ULANE = 32;      // sites per block of the link-field layout
 enum { POT_QUARTIC = 0, POT_MULTI = 1 };
+// Multi-invariant potential superoperator A[(r*d+q)][(i*d+j)], nonzeros only: CSR over
+// the row pairs rq = r*d + q, column pair ij packed as i | j << 8, values in the
+// precision of the arithmetic that reads them (double2 or float2).
+struct PotA { const int* ptr; const unsigned short* ij; const void* v; };
 constexpr int POT_DMAX = 32;   // largest representation the multi-invariant potential accepts
 
 // Programmatic dependent launch: kernels of the MD path are launched so that the
@@ -68,10 +72,13 @@ struct Work { int lat, mu, s0, n; };
 
 struct GenTables {                 // general irrep (src/rep/rep_general.hpp), sparse
   int d, n, dimT, ng;
-  int powN[16];
+  int powN[18];
   const int* wt_ptr; const int* wt_l; const double2* wt_v;   // lift: CSR over tensor index
   const int* w_ptr;  const int* w_i;  const double2* w_v;    // project: CSR over basis vector
   const int* t_ptr;  const int* t_j;  const double2* t_v;    // T^a_R: CSR over (a, row)
+  // single-row irreps: D(U) in closed form (host term lists, gh_sympow.h); null: tensor path
+  const int* sp_ptr; const double2* sp_c; const unsigned char* sp_e;
+  int warp_bytes;                                            // shared memory of one warp
 };
 
 template <typename R> struct V2;
@@ -215,7 +222,7 @@ struct KickArgs {
   double* out;        // M_WRITE destination (SoA like P / like phi, FP64)
   int pot;            // POT_QUARTIC or POT_MULTI
   double mu2;         // multi-invariant potential: -mu2 phi^dag phi
-  const void* asup;   // multi-invariant potential: A = sum_c 2 f_c P_c in the field precision
+  PotA sa;            // multi-invariant potential: A = sum_c 2 f_c P_c, values in the field precision
 };
 
 // The direction is a template parameter so that every index into the lattice
@@ -301,32 +308,32 @@ __device__ __forceinline__ void kick_link(const KickArgs& a, const LatDev& L, in
 // with M = phi phi^dag and A = sum_c 2 f_c P_c the combined channel superoperator
 // ((d^2) x (d^2), vec index i*d + j),
 //   w = A(M) phi,  dV/dphi^* = -mu2 phi + w,  V = -mu2 phi^dag phi + Re(phi^dag w) / 2.
-// Writes w (when given) and returns V.  One thread per site; d^4 complex
-// multiply-adds with A read through L1 (all threads of a warp read the same entry).
+// Writes w (when given) and returns V.  One thread per site; A is held sparse (the
+// weight of the Cartan generators is conserved, so 75-95% of its d^4 entries
+// vanish: 1469 of 28561 for SU(2){12}), read through L1 (every thread of a warp
+// reads the same entry).
 // ---------------------------------------------------------------------------
 template <typename C, typename R>
-__device__ __noinline__ C pot_multi(const R* phi, const LatDev& L, int d, int s, const typename V2<C>::t* __restrict__ A,
-                                    C mu2, cx<C>* w) {
+__device__ __noinline__ C pot_multi(const R* phi, const LatDev& L, int d, int s, const PotA A, C mu2, cx<C>* w) {
+  typedef typename V2<C>::t VT;
+  const VT* __restrict__ av = reinterpret_cast<const VT*>(A.v);
   cx<C> p[POT_DMAX];
   C n2 = C(0);
   for (int k = 0; k < d; ++k) {
     p[k] = ldc<C>(phi, f_index(L, d, k, s));
     n2 += norm2(p[k]);
   }
-  const int dd = d * d;
   C re = C(0);
   for (int r = 0; r < d; ++r) {
     cx<C> acc = zero<C>();
     for (int q = 0; q < d; ++q) {
-      const typename V2<C>::t* row = A + (size_t)(r * d + q) * dd;
+      const int b = __ldg(A.ptr + r * d + q), e = __ldg(A.ptr + r * d + q + 1);
+      if (b == e) continue;
       cx<C> y = zero<C>();                 // A(M)_rq = sum_ij A_{rq,ij} phi_i conj(phi_j)
-      for (int i = 0; i < d; ++i) {
-        cx<C> t = zero<C>();
-        for (int j = 0; j < d; ++j) {
-          const typename V2<C>::t av = __ldg(row + i * d + j);
-          t = cfma_cj(t, p[j], mk<C>(av.x, av.y));
-        }
-        y = cfma(y, p[i], t);
+      for (int z = b; z < e; ++z) {
+        const int ij = __ldg(A.ij + z);
+        const VT a = __ldg(av + z);
+        y = cfma(y, mk<C>(a.x, a.y), mulc(p[ij & 0xFF], p[ij >> 8]));
       }
       acc = cfma(acc, y, p[q]);
     }
@@ -350,7 +357,7 @@ __device__ __forceinline__ void kick_site(const KickArgs& a, const LatDev& L, in
     for (int k = 0; k < d; ++k) { v[k] = ldc<C>(phi, f_index(L, d, k, s)); n2 += norm2(v[k]); }
     if (a.pot == POT_MULTI) {          // -2 dV/dphi^* = 2 mu2 phi - 2 A(M) phi
       cx<C> w[d];
-      pot_multi<C, R>(phi, L, d, s, (const typename V2<C>::t*)a.asup, (C)a.mu2, w);
+      pot_multi<C, R>(phi, L, d, s, a.sa, (C)a.mu2, w);
 #pragma unroll
       for (int k = 0; k < d; ++k) F[k] = sub(scale(v[k], C(2) * (C)a.mu2), scale(w[k], C(2)));
     } else {                           // -2 dV/dphi^* = -2 [1 + 2 lambda (n2 - 1)] phi
@@ -396,7 +403,7 @@ __device__ __forceinline__ void kick_site(const KickArgs& a, const LatDev& L, in
     for (int k = 0; k < d; ++k) n2 += norm2(ldc<C>(phi, f_index(L, d, k, s)));
     const C cc = C(1) + C(2) * (C)L.lambda * (n2 - C(1));
     cx<C> w[POT_DMAX];
-    if (a.pot == POT_MULTI) pot_multi<C, R>(phi, L, d, s, (const typename V2<C>::t*)a.asup, (C)a.mu2, w);
+    if (a.pot == POT_MULTI) pot_multi<C, R>(phi, L, d, s, a.sa, (C)a.mu2, w);
     int yb[D];
 #pragma unroll
     for (int mu = 0; mu < D; ++mu) yb[mu] = nbwd(L, s, x[mu], mu);
@@ -461,6 +468,9 @@ __global__ void __launch_bounds__(KICK_BLOCK, KickMinBlocks<R>::v) k_kick(const 
 // the basis W, apply U on each of the n slots, project with W^dag), but W and
 // T^a_R are held sparse (97% / 94% zeros for the SU(3) 27-plet) and the lanes of
 // the warp split the tensor index / slot fibres / basis vectors between them.
+// Single-row irreps whose term list the host built (GenTables::sp_ptr) take D(U)
+// in closed form instead (sympow_matrix: the lanes split the d*d entries), then
+// two d x d matrix-vector products.
 //   mode 0: psi_f = D phi_{x+mu}, psi_b = D^dag phi_x -> scratch; P -= eps F_matter
 //   mode 1: psi_f only (for the scalar action and the link energy)
 //   mode 2: F_matter -> out (no P update), psi_f, psi_b -> scratch
@@ -524,6 +534,40 @@ __device__ void gen_apply(const GenTables& t, const Mat<N, C>& M, bool dag, cons
   __syncwarp();
 }
 
+// D(U) of a single-row irrep from its term list, FP64, one warp:
+//   D[k][l] = sum_terms c prod_ij U_ij^K_ij
+// with the powers U_ij^p (p = 0..n) tabulated first.  Dm: d*d, Pw: N*N*(n+1) entries
+// of this warp's shared memory.
+template <int N, typename C>
+__device__ void sympow_matrix(const GenTables& t, const Mat<N, C>& M, cx<double>* Dm, cx<double>* Pw, int lane) {
+  const int n = t.n, d = t.d;
+  if (lane < N * N) {
+    const cx<double> u = mk<double>((double)M.e[lane].re, (double)M.e[lane].im);
+    cx<double> p = mk<double>(1.0, 0.0);
+    for (int q = 0; q <= n; ++q) {
+      Pw[lane * (n + 1) + q] = p;
+      p = mul(p, u);
+    }
+  }
+  __syncwarp();
+  for (int e = lane; e < d * d; e += 32) {
+    cx<double> acc = zero<double>();
+    for (int q = t.sp_ptr[e]; q < t.sp_ptr[e + 1]; ++q) {
+      const double2 c = t.sp_c[q];
+      cx<double> pr = mk<double>(c.x, c.y);
+      const unsigned char* ex = t.sp_e + (size_t)q * (N * N);
+#pragma unroll
+      for (int ij = 0; ij < N * N; ++ij) {
+        const int k = ex[ij];
+        if (k) pr = mul(pr, Pw[ij * (n + 1) + k]);
+      }
+      acc = add(acc, pr);
+    }
+    Dm[e] = acc;
+  }
+  __syncwarp();
+}
+
 template <int D, int N, typename R>
 __global__ void __launch_bounds__(GEN_WARPS * 32) k_gen_links(const GenArgs a) {
   pdl_enter();
@@ -535,9 +579,14 @@ __global__ void __launch_bounds__(GEN_WARPS * 32) k_gen_links(const GenArgs a) {
   const LatDev L = a.lats[w.lat];
   const int mu = w.mu, s = w.s0 + warp;
   const int d = a.t.d, dimT = a.t.dimT;
-  cx<C>* base = reinterpret_cast<cx<C>*>(smem_raw) + (size_t)warp * (dimT + 4 * d);
-  cx<C>* buf = base;
-  cx<C>* px = buf + dimT;
+  // this warp's shared memory: tensor path [buf: dimT][px py pf pb: d each];
+  // closed-form path [Dm: d*d][Pw: N*N*(n+1)] (FP64) then [px py pf pb]
+  unsigned char* wbase = smem_raw + (size_t)warp * a.t.warp_bytes;
+  const bool sp = a.t.sp_ptr != nullptr;
+  cx<double>* Dm = reinterpret_cast<cx<double>*>(wbase);
+  cx<double>* Pw = Dm + d * d;
+  cx<C>* buf = reinterpret_cast<cx<C>*>(wbase);
+  cx<C>* px = sp ? reinterpret_cast<cx<C>*>(Pw + N * N * (a.t.n + 1)) : buf + dimT;
   cx<C>* py = px + d;
   cx<C>* pf = py + d;
   cx<C>* pb = pf + d;
@@ -552,8 +601,22 @@ __global__ void __launch_bounds__(GEN_WARPS * 32) k_gen_links(const GenArgs a) {
     py[k] = ldc<C>(phi, f_index(L, d, k, spm));
   }
   __syncwarp();
-  gen_apply<N, C>(a.t, M, false, py, buf, pf, lane);
-  if (a.mode != 1) gen_apply<N, C>(a.t, M, true, px, buf, pb, lane);
+  if (sp) {
+    sympow_matrix<N, C>(a.t, M, Dm, Pw, lane);
+    for (int k = lane; k < d; k += 32) {
+      cx<double> f = zero<double>(), b = zero<double>();
+      for (int l = 0; l < d; ++l) {
+        f = cfma(f, Dm[k * d + l], mk<double>((double)py[l].re, (double)py[l].im));
+        b = cfma_cj(b, Dm[l * d + k], mk<double>((double)px[l].re, (double)px[l].im));
+      }
+      pf[k] = mk<C>((C)f.re, (C)f.im);
+      pb[k] = mk<C>((C)b.re, (C)b.im);
+    }
+    __syncwarp();
+  } else {
+    gen_apply<N, C>(a.t, M, false, py, buf, pf, lane);
+    if (a.mode != 1) gen_apply<N, C>(a.t, M, true, px, buf, pb, lane);
+  }
   R* psif = (R*)a.psif;
   R* psib = (R*)a.psib;
   for (int k = lane; k < d; k += 32) {
@@ -779,7 +842,7 @@ struct MeasArgs {
   const void* psif;
   int pot;
   double mu2;
-  const double2* asup;   // multi-invariant potential superoperator (FP64)
+  PotA sa;               // multi-invariant potential superoperator (FP64 values)
   int d;
   int scalar;
   double* partials;   // [block][NRED]
@@ -833,7 +896,7 @@ __global__ void __launch_bounds__(KBLOCK) k_measure(const MeasArgs a) {
         r[4] += norm2(ldc<double>(pi, f_index(L, a.d, k, s)));
       }
       r[5] = n2;
-      r[1] = (a.pot == POT_MULTI) ? pot_multi<double, R>(phi, L, a.d, s, a.asup, a.mu2, nullptr)
+      r[1] = (a.pot == POT_MULTI) ? pot_multi<double, R>(phi, L, a.d, s, a.sa, a.mu2, nullptr)
                                   : n2 + L.lambda * (n2 - 1.0) * (n2 - 1.0);
       if (REP == REP_FUND || REP == REP_ADJ) {
         constexpr int d = RepDim<N, REP>::d;

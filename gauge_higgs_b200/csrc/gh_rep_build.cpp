@@ -172,7 +172,7 @@ int setup(Builder& b, int N, const int* rows, int nrows) {
   for (size_t i = 0; i + 1 < b.rows.size(); ++i) if (b.rows[i] < b.rows[i + 1]) return GH_ERR_REP;
   if ((int)b.rows.size() > N - 1) return GH_ERR_REP;
   b.n = std::accumulate(b.rows.begin(), b.rows.end(), 0);
-  if (b.n > 15) return GH_ERR_REP;
+  if (b.n > 17) return GH_ERR_REP;        // N^n <= 200000 below bounds n by 17 (SU(2))
   b.powN.assign(b.n + 1, 1);
   for (int k = 1; k <= b.n; ++k) b.powN[k] = b.powN[k - 1] * N;
   b.dimT = b.powN[b.n];

@@ -125,6 +125,17 @@ class GeneralRep(Representation):
     def young_rows(self):
         return list(self.rows)
 
+    def closed_form_matrix(self, U):
+        """D(U) of a single-row irrep in closed form (host; gh_sympow_matrix), with the
+        number of monomial terms; raises GaugeHiggsError for irreps without one."""
+        U = np.ascontiguousarray(U, np.complex128)
+        Dm = np.zeros((self.d, self.d), np.complex128)
+        nt = C.c_long()
+        r = self.desc()
+        check(LIB.gh_sympow_matrix(self.N, C.byref(r), _dptr(U.view(np.float64)), _dptr(Dm.view(np.float64)),
+                                   C.byref(nt)))
+        return Dm, nt.value
+
     def name(self):
         return "general[" + ",".join(map(str, self.rows)) + "]"
 
@@ -486,6 +497,13 @@ class Ensemble:
         self.ctx("gh_temper_stats", att.ctypes.data_as(C.POINTER(C.c_uint64)),
                  acc.ctypes.data_as(C.POINTER(C.c_uint64)), _dptr(kap))
         return att, acc, kap
+
+    def rep_path(self):
+        """How the device applies D(U): "register" (fundamental, adjoint), "tensor"
+        (general irreps) or "closed_form" (large single-row irreps)."""
+        p = C.c_int()
+        self.ctx("gh_rep_path", C.byref(p))
+        return {0: "register", 1: "tensor", 2: "closed_form"}[p.value]
 
     def device_bytes(self):
         b = C.c_uint64()

@@ -46,6 +46,8 @@ extern "C" {
 enum { GH_REP_NONE = 0, GH_REP_FUND = 1, GH_REP_ADJ = 2, GH_REP_GENERAL = 3 };
 enum { GH_PREC_FP64 = 0, GH_PREC_FP32_MD = 1 };
 enum { GH_LEAPFROG = 0, GH_OMELYAN = 1 };
+/* How D(U) of the scalar's representation is applied on the device (gh_rep_path). */
+enum { GH_PATH_REGISTER = 0, GH_PATH_TENSOR = 1, GH_PATH_CLOSED_FORM = 2 };
 
 /* Representation R of the scalar.  Replaces the Representation<N> object
  * (src/rep/representation.hpp:12-32).  GENERAL carries the host-built tables of
@@ -273,6 +275,26 @@ double gh_rng_gauss(uint64_t seed, uint64_t key);
  * rows: Young diagram row lengths. */
 int gh_rep_general_info(int N, const int* rows, int nrows, int* d, int* n_boxes, long* dimT);
 int gh_rep_general_build(int N, const int* rows, int nrows, double* T, double* W);
+
+/* ---- general irreps: how D(U) is applied ----
+ * Fundamental and adjoint: in registers (GH_PATH_REGISTER).  A general irrep uses
+ * the exact tensor construction <W_k| U^(x)n |W_l> (GH_PATH_TENSOR;
+ * src/rep/rep_general.hpp:122-131,184-220), except for a single-row Young diagram
+ * {n}, whose basis vectors are symmetrised multisets: there the context builds D(U)
+ * per link in closed form, a sum of monomials in the entries of U
+ * (GH_PATH_CLOSED_FORM), when that takes fewer operations than the tensor path or
+ * when the N^n tensor does not fit in shared memory.  It replaces the reference's
+ * GeneralRep fast path exp(i w.T_R) (src/rep/rep_general.hpp:94-112,165-179),
+ * which that code enables for the same large single-row irreps (SU(2){12}: d = 13,
+ * N^n = 4096); the closed form is the tensor matrix itself, not an approximation
+ * of it, and the context checks it against the tensor construction on two test
+ * links before using it.
+ * gh_rep_path: the path a context uses.
+ * gh_sympow_matrix: host-only evaluation of the closed form D(U) (U: N x N complex
+ *   row-major; D: d x d complex) and the number of terms; GH_ERR_REP when the
+ *   irrep has no closed form (message through gh_last_error(NULL)). */
+int gh_rep_path(const gh_ctx* ctx, int* path);
+int gh_sympow_matrix(int N, const gh_rep_desc* rep, const double* U, double* D, long* n_terms);
 
 /* ---- multi-invariant onsite potential ----
  * V[phi] = -mu2 phi^dag phi + sum_c f_c Tr(M^dag P_c M), M = phi phi^dag, P_c the

@@ -425,6 +425,7 @@ class Reference:
         L.ref_session_create.argtypes = [C.c_int, C.c_int, _ip, C.c_char_p, C.c_double, C.c_double, C.c_double,
                                          C.c_int, C.c_double, _u64, C.c_int, C.c_double, C.c_double]
         L.ref_session_run.argtypes = [C.c_void_p, C.c_int, _dp]
+        L.ref_session_set_multi.argtypes = [C.c_void_p, _dp, C.c_int, C.c_double]
         L.ref_session_acceptance.restype = C.c_double
         L.ref_session_acceptance.argtypes = [C.c_void_p]
         L.ref_session_destroy.argtypes = [C.c_void_p]
@@ -666,6 +667,14 @@ class RefSession:
         out = np.zeros((max(ntraj, 1), 5)) if series else None
         self.lib.ref_session_run(self.h, ntraj, _d(out) if series else None)
         return out[:ntraj] if series else None
+
+    def set_multi(self, f, mu2):
+        """Install the multi-invariant potential (couplings f, one per channel; mu2), as
+        hmc_higgs_multi does (src/hmc_higgs_multi.cpp:51-80)."""
+        f = np.ascontiguousarray(f, np.float64)
+        rc = self.lib.ref_session_set_multi(self.h, _d(f), len(f), mu2)
+        if rc:
+            raise RuntimeError(f"ref_session_set_multi rc={rc}")
 
     def acceptance(self):
         return self.lib.ref_session_acceptance(self.h)

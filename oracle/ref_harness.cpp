@@ -369,6 +369,7 @@ struct RefSession {
   virtual ~RefSession() {}
   virtual int run(int ntraj, double* series) = 0;   // series: [ntraj][5] as ref_run
   virtual double acceptance() = 0;
+  virtual int set_multi(const double* f, int nf, double mu2) = 0;   // nf must equal the channel count
 };
 template <int DD, int NN>
 struct RefSessionT : RefSession {
@@ -387,6 +388,16 @@ struct RefSessionT : RefSession {
     return 0;
   }
   double acceptance() override { return h.acceptance(); }
+  // the reference driver's potential set-up (src/hmc_higgs_multi.cpp:51-80)
+  std::unique_ptr<CasimirChannels<NN>> ch;
+  std::unique_ptr<MultiInvariantPotential<NN>> pot;
+  int set_multi(const double* f, int nf, double mu2) override {
+    ch.reset(new CasimirChannels<NN>(*r));
+    if (nf != ch->n_channels()) return -3;
+    pot.reset(new MultiInvariantPotential<NN>(*ch, std::vector<Real>(f, f + nf), mu2));
+    h.potential = pot.get();
+    return 0;
+  }
 };
 
 extern "C" {
@@ -403,6 +414,9 @@ void* ref_session_create(int D, int N, const int* L, const char* spec, double be
   return s;
 }
 int ref_session_run(void* s, int ntraj, double* series) { return s ? static_cast<RefSession*>(s)->run(ntraj, series) : -1; }
+int ref_session_set_multi(void* s, const double* f, int nf, double mu2) {
+  return s ? static_cast<RefSession*>(s)->set_multi(f, nf, mu2) : -1;
+}
 double ref_session_acceptance(void* s) { return s ? static_cast<RefSession*>(s)->acceptance() : 0.0; }
 void ref_session_destroy(void* s) { delete static_cast<RefSession*>(s); }
 
