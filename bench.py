@@ -464,7 +464,7 @@ def run_extra(a, dist):
                 h.potential = gh.MultiInvariantPotential(gh.CasimirChannels(rep), f2i, 0.065)
                 h.hot(0.8)
                 h.phi_gaussian(12345, 0.3)
-                v, rec = gpu_rate(h, 40 if Lx == 4 else 10, W=2)
+                v, rec = gpu_rate(h, 100 if Lx == 4 else 40, W=30)
                 cpu = None
                 if prec == "fp64" and Lx == 4 and ref is not None:
                     s = RefSession(ref, 4, 2, [Lx] * 4, "12", 2.0, 0.1, 0.5, 20, 1.0, 1, OMELYAN, 0.8, 0.3)

@@ -576,7 +576,9 @@ int gh_ctx_create(int D, int N, int n_lat, const int* L, const gh_rep_desc* rep,
       { g_err = ctx->err; return rc; }
   }
   if (ctx->rep == REP_GEN) {
-    if ((rc = dalloc(ctx, &psif, (size_t)g * 2 * rs)) || (rc = dalloc(ctx, &psib, (size_t)g * 2 * rs))) { g_err = ctx->err; return rc; }
+    if ((rc = dalloc(ctx, &psif, (size_t)g * 2 * rs)) || (rc = dalloc(ctx, &psib, (size_t)g * 2 * rs)) ||
+        (rc = dalloc(ctx, &ctx->b.wpot, (size_t)std::max<long long>(f, 1))))
+      { g_err = ctx->err; return rc; }
     if ((rc = build_general(ctx, rep))) { g_err = ctx->err; return rc; }
   }
   b.U = U; b.Us = Us; b.P = P; b.phi = phi; b.phis = phis; b.pi = pi; b.psif = psif; b.psib = psib;

@@ -45,6 +45,7 @@ struct Bufs {
   int pot;               // POT_QUARTIC or POT_MULTI
   double mu2;
   PotA sa64, sa32;       // multi-invariant potential superoperator, FP64 and FP32 values
+  double2* wpot;         // general irreps: w = A(M) phi per site (FP64, laid out like phi)
   cudaStream_t st;
 };
 
@@ -83,6 +84,7 @@ struct Engine : EngineBase {
     a.eps = eps; a.mode = mode; a.flags = flags; a.d = b.d; a.out = out;
     a.pot = b.pot; a.mu2 = b.mu2;
     a.sa = sizeof(R) == sizeof(double) ? b.sa64 : b.sa32;
+    a.wpot = b.wpot;
     const bool do_sites = sites && b.scalar;
     const int first = links ? 0 : b.nwk_links;
     const int count = (links ? b.nwk_links : 0) + (do_sites ? b.nwk_sites : 0);
@@ -95,6 +97,7 @@ struct Engine : EngineBase {
     GenArgs a;
     a.work = b.w_gen; a.lats = b.lats; a.U = b.U; a.P = b.P; a.phi = b.phi; a.psif = b.psif; a.psib = b.psib;
     a.t = b.gen; a.eps = eps; a.mode = mode; a.out = out;
+    a.pot = b.pot; a.sa = b.sa64; a.wpot = b.wpot;
     const size_t sm = gen_smem(b);
     launch(k_gen_links<D, N, R>, b.nw_gen, b.gen_warps * 32, sm, b.st, a);
   }
@@ -120,7 +123,7 @@ struct Engine : EngineBase {
     MeasArgs a;
     a.work = b.w_all + b.nw_links; a.lats = b.lats; a.U = b.U; a.P = b.P; a.phi = b.phi; a.pi = b.pi;
     a.psif = b.psif; a.d = b.d; a.scalar = b.scalar; a.partials = b.partials;
-    a.pot = b.pot; a.mu2 = b.mu2; a.sa = b.sa64;
+    a.pot = b.pot; a.mu2 = b.mu2; a.sa = b.sa64; a.wpot = b.wpot;
     launch(k_measure<D, N, R, REP>, b.nw_sites, KBLOCK, 0, b.st, a);
   }
   void init(const Bufs& b, InitArgs a, bool links, bool sites) override {

@@ -223,6 +223,7 @@ struct KickArgs {
   int pot;            // POT_QUARTIC or POT_MULTI
   double mu2;         // multi-invariant potential: -mu2 phi^dag phi
   PotA sa;            // multi-invariant potential: A = sum_c 2 f_c P_c, values in the field precision
+  const double2* wpot;  // general irreps: w = A(M) phi per site, written by k_gen_links
 };
 
 // The direction is a template parameter so that every index into the lattice
@@ -402,14 +403,18 @@ __device__ __forceinline__ void kick_site(const KickArgs& a, const LatDev& L, in
     C n2 = C(0);
     for (int k = 0; k < d; ++k) n2 += norm2(ldc<C>(phi, f_index(L, d, k, s)));
     const C cc = C(1) + C(2) * (C)L.lambda * (n2 - C(1));
-    cx<C> w[POT_DMAX];
-    if (a.pot == POT_MULTI) pot_multi<C, R>(phi, L, d, s, a.sa, (C)a.mu2, w);
     int yb[D];
 #pragma unroll
     for (int mu = 0; mu < D; ++mu) yb[mu] = nbwd(L, s, x[mu], mu);
     for (int k = 0; k < d; ++k) {
       const cx<C> pk = ldc<C>(phi, f_index(L, d, k, s));
-      cx<C> F = (a.pot == POT_MULTI) ? sub(scale(pk, C(2) * (C)a.mu2), scale(w[k], C(2))) : scale(pk, C(-2) * cc);
+      cx<C> F;
+      if (a.pot == POT_MULTI) {
+        const double2 wk = a.wpot[f_index(L, d, k, s)];
+        F = sub(scale(pk, C(2) * (C)a.mu2), scale(mk<C>((C)wk.x, (C)wk.y), C(2)));
+      } else {
+        F = scale(pk, C(-2) * cc);
+      }
 #pragma unroll
       for (int mu = 0; mu < D; ++mu) {
         
@@ -488,6 +493,9 @@ struct GenArgs {
   double eps;
   int mode;
   double* out;
+  int pot;            // POT_MULTI: the warps of mu = 0 also write w = A(M) phi_x
+  PotA sa;            // superoperator rows, FP64 values
+  double2* wpot;      // w per site, FP64, laid out like phi
 };
 
 template <int N, typename C>
@@ -601,6 +609,27 @@ __global__ void __launch_bounds__(GEN_WARPS * 32) k_gen_links(const GenArgs a) {
     py[k] = ldc<C>(phi, f_index(L, d, k, spm));
   }
   __syncwarp();
+  if (a.pot == POT_MULTI && mu == 0) {
+    // multi-invariant potential of site s, one lane per component r (FP64):
+    //   w_r = sum_q sum_ij A_{rq,ij} phi_i conj(phi_j) phi_q
+    const double2* __restrict__ av = reinterpret_cast<const double2*>(a.sa.v);
+    for (int r = lane; r < d; r += 32) {
+      cx<double> acc = zero<double>();
+      for (int q = 0; q < d; ++q) {
+        const int b = __ldg(a.sa.ptr + r * d + q), e = __ldg(a.sa.ptr + r * d + q + 1);
+        if (b == e) continue;
+        cx<double> y = zero<double>();
+        for (int z = b; z < e; ++z) {
+          const int ij = __ldg(a.sa.ij + z);
+          const double2 v = __ldg(av + z);
+          const cx<C> pi = px[ij & 0xFF], pj = px[ij >> 8];
+          y = cfma(y, mk<double>(v.x, v.y), mulc(mk<double>(pi.re, pi.im), mk<double>(pj.re, pj.im)));
+        }
+        acc = cfma(acc, y, mk<double>(px[q].re, px[q].im));
+      }
+      a.wpot[f_index(L, d, r, s)] = make_double2(acc.re, acc.im);
+    }
+  }
   if (sp) {
     sympow_matrix<N, C>(a.t, M, Dm, Pw, lane);
     for (int k = lane; k < d; k += 32) {
@@ -843,6 +872,7 @@ struct MeasArgs {
   int pot;
   double mu2;
   PotA sa;               // multi-invariant potential superoperator (FP64 values)
+  const double2* wpot;   // general irreps: w = A(M) phi per site, written by k_gen_links
   int d;
   int scalar;
   double* partials;   // [block][NRED]
@@ -896,8 +926,19 @@ __global__ void __launch_bounds__(KBLOCK) k_measure(const MeasArgs a) {
         r[4] += norm2(ldc<double>(pi, f_index(L, a.d, k, s)));
       }
       r[5] = n2;
-      r[1] = (a.pot == POT_MULTI) ? pot_multi<double, R>(phi, L, a.d, s, a.sa, a.mu2, nullptr)
-                                  : n2 + L.lambda * (n2 - 1.0) * (n2 - 1.0);
+      if (a.pot != POT_MULTI) {
+        r[1] = n2 + L.lambda * (n2 - 1.0) * (n2 - 1.0);
+      } else if (REP == REP_GEN) {         // V = -mu2 phi^dag phi + Re(phi^dag w) / 2, w from k_gen_links
+        double re = 0.0;
+        for (int k = 0; k < a.d; ++k) {
+          const cx<double> pk = ldc<double>(phi, f_index(L, a.d, k, s));
+          const double2 wk = a.wpot[f_index(L, a.d, k, s)];
+          re = fmad(pk.re, wk.x, fmad(pk.im, wk.y, re));
+        }
+        r[1] = -a.mu2 * n2 + 0.5 * re;
+      } else {
+        r[1] = pot_multi<double, R>(phi, L, a.d, s, a.sa, a.mu2, nullptr);
+      }
       if (REP == REP_FUND || REP == REP_ADJ) {
         constexpr int d = RepDim<N, REP>::d;
         cx<double> px[d], py[d], o[d];
