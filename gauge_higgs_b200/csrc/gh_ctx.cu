@@ -62,7 +62,7 @@ struct gh_ctx {
   // the tensor path or when the tensor buffer does not fit in shared memory)
   ghsym::Terms sp;
   bool use_sp = false;
-  size_t gen_warp_bytes = 0;
+  size_t gen_warp_bytes = 0, gen_px_off = 0;
   // multi-invariant potential: device copies of the channel superoperator (sparse rows)
   int* sa_ptr = nullptr;
   unsigned short* sa_ij = nullptr;
@@ -433,6 +433,7 @@ int build_general(gh_ctx* ctx, const gh_rep_desc* r) {
   t.wt_ptr = p1; t.wt_l = p2; t.wt_v = v1; t.w_ptr = p3; t.w_i = p4; t.w_v = v2; t.t_ptr = p5; t.t_j = p6; t.t_v = v3;
   t.sp_ptr = nullptr; t.sp_c = nullptr; t.sp_e = nullptr;
   t.warp_bytes = (int)ctx->gen_warp_bytes;
+  t.px_off = (int)ctx->gen_px_off;
   if (ctx->use_sp) {
     const ghsym::Terms& q = ctx->sp;
     int* sptr;
@@ -543,11 +544,17 @@ int gh_ctx_create(int D, int N, int n_lat, const int* L, const gh_rep_desc* rep,
         ctx->use_sp = term_ops < tensor_ops || tensor_warp > 227 * 1024;
       }
     }
-    size_t per_warp = ctx->use_sp
-        ? ((size_t)rep->d * rep->d + (size_t)N * N * (rep->n_boxes + 1)) * 16 + 4 * (size_t)rep->d * cs
-        : tensor_warp;
+    // a warp's region: [tensor buffer, or D(U) and the powers of U's entries][px py pf pb];
+    // the first part also holds the matter force's (a, row) partial sums (ng*d
+    // doubles) after it is used, and A(M) of the potential before, where that fits
+    size_t region = ctx->use_sp ? ((size_t)rep->d * rep->d + (size_t)N * N * (rep->n_boxes + 1)) * 16
+                                : (size_t)rep->dimT * cs;
+    region = std::max(region, (size_t)(N * N - 1) * rep->d * 8);
+    region = (region + 15) / 16 * 16;
+    size_t per_warp = region + 4 * (size_t)rep->d * cs;
     per_warp = (per_warp + 15) / 16 * 16;
     ctx->gen_warp_bytes = per_warp;
+    ctx->gen_px_off = region;
     while (gw > 1 && gw * per_warp > 227 * 1024) gw /= 2;
     if (per_warp > 227 * 1024) return fail(nullptr, GH_ERR_REP, "general irrep too large for the shared-memory tensor buffer");
     for (int l = 0; l < n_lat; ++l)

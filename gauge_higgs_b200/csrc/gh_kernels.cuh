@@ -79,6 +79,7 @@ struct GenTables {                 // general irrep (src/rep/rep_general.hpp), s
   // single-row irreps: D(U) in closed form (host term lists, gh_sympow.h); null: tensor path
   const int* sp_ptr; const double2* sp_c; const unsigned char* sp_e;
   int warp_bytes;                                            // shared memory of one warp
+  int px_off;                                                // byte offset of px in a warp's region
 };
 
 template <typename R> struct V2;
@@ -594,7 +595,10 @@ __global__ void __launch_bounds__(GEN_WARPS * 32) k_gen_links(const GenArgs a) {
   cx<double>* Dm = reinterpret_cast<cx<double>*>(wbase);
   cx<double>* Pw = Dm + d * d;
   cx<C>* buf = reinterpret_cast<cx<C>*>(wbase);
-  cx<C>* px = sp ? reinterpret_cast<cx<C>*>(Pw + N * N * (a.t.n + 1)) : buf + dimT;
+  // the region before px (the tensor buffer or D and the powers) also holds, before it
+  // is filled, A(M) of the potential (d*d FP64 complex) where that fits, and, after,
+  // the matter force's partial sums (ng*d doubles, which the host makes room for)
+  cx<C>* px = reinterpret_cast<cx<C>*>(wbase + a.t.px_off);
   cx<C>* py = px + d;
   cx<C>* pf = py + d;
   cx<C>* pb = pf + d;
@@ -610,25 +614,35 @@ __global__ void __launch_bounds__(GEN_WARPS * 32) k_gen_links(const GenArgs a) {
   }
   __syncwarp();
   if (a.pot == POT_MULTI && mu == 0) {
-    // multi-invariant potential of site s, one lane per component r (FP64):
-    //   w_r = sum_q sum_ij A_{rq,ij} phi_i conj(phi_j) phi_q
+    // multi-invariant potential of site s (FP64):
+    //   A(M)_rq = sum_ij A_{rq,ij} phi_i conj(phi_j),  w_r = sum_q A(M)_rq phi_q.
+    // Where A(M) fits in the region before px (always on the closed-form path) the
+    // lanes split the row pairs rq, then one lane per r sums over q; otherwise one
+    // lane per r does both.  Fixed summation order either way.
     const double2* __restrict__ av = reinterpret_cast<const double2*>(a.sa.v);
+    const bool split = (size_t)d * d * sizeof(cx<double>) <= (size_t)a.t.px_off;
+    cx<double>* AM = reinterpret_cast<cx<double>*>(wbase);
+    auto am = [&](int rq) {
+      const int b = __ldg(a.sa.ptr + rq), e = __ldg(a.sa.ptr + rq + 1);
+      cx<double> y = zero<double>();
+      for (int z = b; z < e; ++z) {
+        const int ij = __ldg(a.sa.ij + z);
+        const double2 v = __ldg(av + z);
+        const cx<C> pi = px[ij & 0xFF], pj = px[ij >> 8];
+        y = cfma(y, mk<double>(v.x, v.y), mulc(mk<double>(pi.re, pi.im), mk<double>(pj.re, pj.im)));
+      }
+      return y;
+    };
+    if (split) {
+      for (int rq = lane; rq < d * d; rq += 32) AM[rq] = am(rq);
+      __syncwarp();
+    }
     for (int r = lane; r < d; r += 32) {
       cx<double> acc = zero<double>();
-      for (int q = 0; q < d; ++q) {
-        const int b = __ldg(a.sa.ptr + r * d + q), e = __ldg(a.sa.ptr + r * d + q + 1);
-        if (b == e) continue;
-        cx<double> y = zero<double>();
-        for (int z = b; z < e; ++z) {
-          const int ij = __ldg(a.sa.ij + z);
-          const double2 v = __ldg(av + z);
-          const cx<C> pi = px[ij & 0xFF], pj = px[ij >> 8];
-          y = cfma(y, mk<double>(v.x, v.y), mulc(mk<double>(pi.re, pi.im), mk<double>(pj.re, pj.im)));
-        }
-        acc = cfma(acc, y, mk<double>(px[q].re, px[q].im));
-      }
+      for (int q = 0; q < d; ++q) acc = cfma(acc, split ? AM[r * d + q] : am(r * d + q), mk<double>(px[q].re, px[q].im));
       a.wpot[f_index(L, d, r, s)] = make_double2(acc.re, acc.im);
     }
+    __syncwarp();
   }
   if (sp) {
     sympow_matrix<N, C>(a.t, M, Dm, Pw, lane);
@@ -654,20 +668,24 @@ __global__ void __launch_bounds__(GEN_WARPS * 32) k_gen_links(const GenArgs a) {
     if (a.mode != 1) stc<C>(psib, gi, pb[k]);
   }
   if (a.mode == 1) return;
-  // matter force: g^a = -2 Im(phi_x^dag T^a_R psi_f), F^a = -kappa g^a
+  // matter force: g^a = -2 Im(phi_x^dag T^a_R psi_f), F^a = -kappa g^a.  The lanes
+  // split the (a, row) pairs; the rows of each a are then summed in order.
   constexpr int ng = N * N - 1;
-  for (int g = lane; g < ng; g += 32) {
-    cx<C> z = zero<C>();
-    for (int i = 0; i < d; ++i) {
-      cx<C> ti = zero<C>();
-      const int r = g * d + i;
-      for (int p = a.t.t_ptr[r]; p < a.t.t_ptr[r + 1]; ++p) {
-        const double2 tv = a.t.t_v[p];
-        ti = cfma(ti, mk<C>((C)tv.x, (C)tv.y), pf[a.t.t_j[p]]);
-      }
-      z = cfma_cj(z, px[i], ti);
+  double* zc = reinterpret_cast<double*>(wbase);
+  for (int r = lane; r < ng * d; r += 32) {
+    const int i = r % d;
+    cx<C> ti = zero<C>();
+    for (int p = a.t.t_ptr[r]; p < a.t.t_ptr[r + 1]; ++p) {
+      const double2 tv = a.t.t_v[p];
+      ti = cfma(ti, mk<C>((C)tv.x, (C)tv.y), pf[a.t.t_j[p]]);
     }
-    const C F = -(C)L.kappa * (C(-2) * z.im);
+    zc[r] = (double)px[i].re * (double)ti.im - (double)px[i].im * (double)ti.re;   // Im(conj(phi_i) t_i)
+  }
+  __syncwarp();
+  for (int g = lane; g < ng; g += 32) {
+    double zim = 0.0;
+    for (int i = 0; i < d; ++i) zim += zc[g * d + i];
+    const C F = -(C)L.kappa * (C(-2) * (C)zim);
     const long long pi_ = p_index(L, ng, mu, g, s);
     if (a.mode == 0) {
       R* P = (R*)a.P;

@@ -136,3 +136,31 @@ def test_unit_couplings_reproduce_quartic_hmc():
     assert np.abs(a["dH"] - b["dH"]).max() < 1e-6
     assert np.abs(a["plaquette"] - b["plaquette"]).max() < 1e-9
     assert np.abs(a["L_phi"] - b["L_phi"]).max() < 1e-9
+
+
+@pytest.mark.parametrize("precision,tol", [("fp64", 1e-12), ("fp32", 2e-5)])
+@pytest.mark.parametrize("N,rows,L", [(3, [2], [3, 2, 2]), (3, [2, 1], [2, 2, 2]), (2, [12], [3, 2, 2])])
+def test_general_irrep_potential_vs_oracle(N, rows, L, precision, tol):
+    """General irreps take w = A(M) phi from the link kernel (both of its lane layouts:
+    the sextet and octet on the tensor path, SU(2){12} on the closed-form path): the
+    scalar force and action against the oracle with the library's superoperator."""
+    import gauge_higgs_b200 as gh
+    from oracle.oracle import Oracle, OracleRep
+    O = Oracle()
+    rep = gh.GeneralRep(N, rows)
+    ch = gh.CasimirChannels(rep)
+    f = np.linspace(0.3, 1.2, ch.n_channels())
+    D = len(L)
+    h = gh.GaugeHiggsHMC(L, rep, seed=4, precision=precision, beta=2.0, kappa=0.17, lam=0.5)
+    h.hot(0.5)
+    h.phi_gaussian(7, 0.6)
+    h.potential = gh.MultiInvariantPotential(ch, f, 0.4)
+    U, phi = h.U, h.phi
+    A = ch.superop(f)
+    orep = OracleRep(O.lib, 3, N, rep.d, int(rep.real), rep.n_boxes, rep.dimT, rep.T, rep.W)
+    ref = O.scalar_force_multi(D, N, L, orep, U, phi, 0.17, A, 0.4)
+    assert np.abs(h.scalar_force() - ref).max() <= tol * np.abs(ref).max()
+    if precision == "fp64":
+        S = O.scalar_action_multi(D, N, L, orep, U, phi, 0.17, A, 0.4)
+        assert abs(h.measure()["S_H"] - S) <= 1e-12 * abs(S)
+    h.close()
