@@ -480,6 +480,58 @@ def run_extra(a, dist):
                             "value": round(v, 2), "unit": "trajectories/s",
                             "acceptance": float(rec["accepted"].mean()), "cpu_baseline": cpu})
                 h.close()
+    if wl in ("scan", "all"):
+        # the reference's wide (beta, kappa) phase scan of the 2I rep at 2^4 (scripts/su2_scan.sh:
+        # beta 1.0..3.0 step 0.25, kappa 0.0..1.0 step 0.1, nmd by its kappa table, tau = 1), which
+        # it runs as 99 single-thread jobs, nproc at a time.  Here each nmd tier is one ensemble
+        # (every point a lattice of it); value = point trajectories per second over all 99 points.
+        f2i = [0.1182, 0.0819, 0.0353, 0.0274, 0.1550, 0.0828, 0.0157, 0.0702, 0.1083, 0.1143, 0.0189, 0.1124, 0.0595]
+        betas = [1.0 + 0.25 * i for i in range(9)]
+        kappas = [0.1 * i for i in range(11)]
+
+        def nmd_for(k):
+            return 16 if k <= 0.21 else 28 if k <= 0.31 else 44 if k <= 0.51 else 56 if k <= 0.71 else 68
+
+        tiers = {}
+        for k in kappas:
+            for b in betas:
+                tiers.setdefault(nmd_for(k), []).append((b, k))
+        for prec in ("fp64", "fp32"):
+            K, total_s, acc = 20, 0.0, []
+            for nmd, pts in sorted(tiers.items()):
+                rep = gh.GeneralRep(2, [12])
+                ens = gh.Ensemble([[2] * 4] * len(pts), rep, seeds=[20260602 + i for i in range(len(pts))], precision=prec,
+                                  beta=[p[0] for p in pts], kappa=[p[1] for p in pts], lam=0.5, nmd=nmd,
+                                  integ="omelyan")
+                ens.potential = gh.MultiInvariantPotential(gh.CasimirChannels(rep), f2i, 0.065)
+                ens.hot(0.8)
+                ens.phi_gaussian(12345, 0.3)
+                v, rec = gpu_rate(ens, K, W=20)
+                total_s += K / v
+                acc.append(float(rec["accepted"].mean()))
+                ens.close()
+            cpu = None
+            if prec == "fp64" and ref is not None:
+                ref.set_threads(1)
+                per_point = 0.0
+                for nmd, pts in sorted(tiers.items()):
+                    b, k = pts[len(pts) // 2]
+                    s = RefSession(ref, 4, 2, [2] * 4, "12", b, k, 0.5, nmd, 1.0, 1, OMELYAN, 0.8, 0.3)
+                    s.set_multi(f2i, 0.065)
+                    s.run(1)
+                    t0 = time.perf_counter()
+                    s.run(3)
+                    per_point += len(pts) * (time.perf_counter() - t0) / 3
+                    s.close()
+                ref.set_threads(cores)
+                cpu = {"value": round(99 * cores / per_point, 3), "cores": cores, "kind": "reference",
+                       "sample": "3 trajectories of one point per nmd tier, one thread; scaled to all 99 points "
+                                 f"run {cores} at a time, as the script's JOBS=nproc"}
+            out.append({"workload": "2I phase scan: SU(2) {12} 2^4, multi-invariant potential, beta 1.0..3.0 x kappa "
+                                    "0.0..1.0 (99 points), Omelyan nmd 16..68 by kappa, one ensemble per nmd tier",
+                        "precision": prec, "value": round(99 * K / total_s, 1),
+                        "unit": "point trajectories/s", "acceptance_by_tier": [round(x, 3) for x in acc],
+                        "cpu_baseline": cpu})
     if wl in ("big", "all"):
         for prec in ("fp64", "fp32"):
             L = [32, 32, 32, 32]
@@ -551,7 +603,7 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--validate-traj", type=int, default=2000)
     ap.add_argument("--validate-therm", type=int, default=200)
-    ap.add_argument("--workload", default="c2", choices=["c2", "c1", "c3", "c4", "big", "stage0", "validate", "all"],
+    ap.add_argument("--workload", default="c2", choices=["c2", "c1", "c3", "c4", "big", "stage0", "scan", "validate", "all"],
                     help="c2 (default) prints the headline line; the others print additional measurements")
     a = ap.parse_args()
     if a.warmup < 3 and a.impl == "ours":

@@ -66,3 +66,22 @@ def test_stage0_point_reversibility(precision, tol):
     h.md_evolve()
     assert max(np.abs(h.U - U0).max(), np.abs(h.phi - phi0).max()) < tol
     h.close()
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_stage0_point_exp_minus_dH(precision):
+    """<exp(-dH)> = 1 and the acceptance at the 2I point kappa = 0.1, nmd = 20, where the
+    reference's own shakedown runs (test/test_scalar.cpp:143-156 gates)."""
+    import gauge_higgs_b200 as gh
+    rep = gh.GeneralRep(2, [12])
+    h = gh.GaugeHiggsHMC([4, 4, 4, 4], rep, seed=3, precision=precision, beta=2.0, kappa=0.1, lam=0.5, nmd=20)
+    h.potential = gh.MultiInvariantPotential(gh.CasimirChannels(rep), F2I, 0.065)
+    h.hot(0.8)
+    h.phi_gaussian(12345, 0.3)
+    h.run(50, records=False)
+    rec = h.run(300)[:, 0]
+    mean = float(np.mean(np.exp(-rec["dH"])))
+    acc = float(np.mean(rec["accepted"]))
+    assert abs(mean - 1.0) < 0.03, (mean, acc)
+    assert acc > 0.9, acc
+    h.close()
