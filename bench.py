@@ -457,13 +457,20 @@ def run_extra(a, dist):
         # the reference's SU(2) -> 2I shakedown point (scripts/su2_stage0.sh: hmc_higgs_multi with
         # rep {12}, d = 13, mu2 = 0.065 and its 13 channel couplings, beta = 2.0, nmd = 20, tau = 1)
         f2i = [0.1182, 0.0819, 0.0353, 0.0274, 0.1550, 0.0828, 0.0157, 0.0702, 0.1083, 0.1143, 0.0189, 0.1124, 0.0595]
-        for Lx in (4, 8):
+        for Lx in [int(x) for x in a.stage0_sizes.split(",")]:
             for prec in ("fp64", "fp32"):
                 rep = gh.GeneralRep(2, [12])
                 h = gh.GaugeHiggsHMC([Lx] * 4, rep, seed=1, precision=prec, beta=2.0, kappa=0.1, lam=0.5, nmd=20)
                 h.potential = gh.MultiInvariantPotential(gh.CasimirChannels(rep), f2i, 0.065)
-                h.hot(0.8)
-                h.phi_gaussian(12345, 0.3)
+                # beyond 4^4 a hot start at nmd = 20 has |dH| >> 1 and the chain never leaves it;
+                # there the driver's GH_COLD start (identity links, phi = 1) is used
+                cold = Lx > 4
+                if cold:
+                    h.cold()
+                    h.phi_cold(1.0)
+                else:
+                    h.hot(0.8)
+                    h.phi_gaussian(12345, 0.3)
                 v, rec = gpu_rate(h, 100 if Lx == 4 else 40, W=30)
                 cpu = None
                 if prec == "fp64" and Lx == 4 and ref is not None:
@@ -476,7 +483,8 @@ def run_extra(a, dist):
                            "sample": "3 trajectories after one"}
                     s.close()
                 out.append({"workload": f"SU(2) {{12}} (d=13) {Lx}^4, multi-invariant potential (13 channels, mu2=0.065), "
-                                        "beta=2.0 kappa=0.1, Omelyan nmd=20, hot start", "precision": prec,
+                                        "beta=2.0 kappa=0.1, Omelyan nmd=20, " + ("cold start" if cold else "hot start"),
+                            "precision": prec,
                             "value": round(v, 2), "unit": "trajectories/s",
                             "acceptance": float(rec["accepted"].mean()), "cpu_baseline": cpu})
                 h.close()
@@ -601,6 +609,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--cpu-traj", type=int, default=3)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--stage0-sizes", default="4,8", help="lattice extents of --workload stage0 (comma list)")
     ap.add_argument("--validate-traj", type=int, default=2000)
     ap.add_argument("--validate-therm", type=int, default=200)
     ap.add_argument("--workload", default="c2", choices=["c2", "c1", "c3", "c4", "big", "stage0", "scan", "validate", "all"],

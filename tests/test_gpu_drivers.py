@@ -80,6 +80,21 @@ def test_hmc_higgs_multi_runs(tmp_path):
     assert r.returncode == 1 and "need 2 couplings" in r.stderr
 
 
+def test_hmc_higgs_multi_2I_scan_point():
+    """One point of the reference's 2I scan (scripts/su2_scan.sh: rep {12}, 2^4, mu2 = 0.065,
+    its 13 couplings, nmd 16 at kappa <= 0.21) through the driver's command line: the
+    closed-form D(U) path end to end, 13 channels, a healthy acceptance."""
+    exe = os.path.join(BIN, "hmc_higgs_multi")
+    coup = "0.1182,0.0819,0.0353,0.0274,0.1550,0.0828,0.0157,0.0702,0.1083,0.1143,0.0189,0.1124,0.0595"
+    r = subprocess.run([exe, "12", "2", "2.0", "0.1", "0.065", coup, "50", "200", "16", "1.0", "20260603"],
+                       capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr
+    assert "13 quartic channels" in r.stdout
+    v = parse(r.stdout)
+    assert v["acceptance"][0] > 0.8
+    assert 0.0 < v["plaquette"][0] < 1.0
+
+
 
 CPP_TEMPER = r'''
 #include <cstdio>

@@ -2,7 +2,9 @@
 matrix the device builds per link for large symmetric irreps, in place of the
 reference's GeneralRep fast path exp(i w.T_R) (src/rep/rep_general.hpp:94-112,165-179).
 Pinned against the oracle's tensor construction (src/rep/rep_general.hpp:122-131)
-and the reference's own rep_matrix (its fast path where it enables one)."""
+and the reference's own rep_matrix (its fast path where it enables one), on the
+irreps of the reference's fast-path test (test/test_repfast.cpp:72-80: SU(2) {6},
+{8}, {12}; SU(3) {2}, {5}) and beyond."""
 import numpy as np
 import pytest
 
@@ -18,7 +20,7 @@ def su(N):
     return Q / np.linalg.det(Q) ** (1.0 / N)
 
 
-@pytest.mark.parametrize("N,n", [(2, 1), (2, 2), (2, 6), (2, 12), (2, 16), (3, 2), (3, 5), (3, 8)])
+@pytest.mark.parametrize("N,n", [(2, 1), (2, 2), (2, 6), (2, 8), (2, 12), (2, 16), (3, 2), (3, 5), (3, 8)])
 def test_closed_form_matches_tensor_construction(N, n):
     import gauge_higgs_b200 as gh
     from oracle.oracle import Oracle, REP_GENERAL
