@@ -39,6 +39,11 @@ METRIC = "SU(3)+Higgs 16^4 trajectories/s, FP32-MD vs FP64 GPU at equal obs; % H
 #   kick  = U 576 + phi 48 + P read+write 512 + pi read+write 96 = 1232 B (FP64), half in FP32
 #   drift = P 256 + U read+write 1152 + pi 48 + phi read+write 96 = 1552 B (FP64), half in FP32
 ALG_BYTES = {"kick": {"fp64": 1232, "fp32": 616}, "drift": {"fp64": 1552, "fp32": 776}}
+# algorithmic flops of one kick per site, SU(3) fundamental, the reference algorithm's count
+# (complex 3x3 matmul 8N^3 - 2N^2 = 198, matrix add 18, generator projection 72):
+#   gauge force 4 links x (13 matmuls + 5 adds + 8 projections) = 12960, matter link force 3080,
+#   scalar force 600, momentum updates 76
+KICK_FLOPS_PER_SITE = 16716
 
 
 def peaks():
@@ -247,6 +252,15 @@ def run_ours(a, dist):
     if os.path.exists(tp):
         with open(tp) as f:
             traffic = json.load(f).get(f"{dom}_fp32_dram_bytes_per_launch")
+    # the kick is arithmetic-heavy: its rate against the FP32 pipe, nominal at the sampled SM clock
+    # (148 SMs x 128 FP32 lanes x 2 flop per FMA)
+    clk = (r.get("clocks") or {}).get("sm_mhz") or 1965.0
+    fp32_peak = 148 * 128 * 2 * clk * 1e6 / 1e12
+    kick_tflops = V * KICK_FLOPS_PER_SITE / (r["kick_ms"] / 1e3) / 1e12
+    compute = {"kernel": "k_kick<4,3,float,FUND>", "flops_per_launch": V * KICK_FLOPS_PER_SITE,
+               "achieved": round(kick_tflops, 2), "peak": round(fp32_peak, 1), "unit": "TFLOP/s",
+               "frac": round(kick_tflops / fp32_peak, 4),
+               "peak_source": "nominal FP32 FMA rate at the sampled SM clock (148 SMs x 128 lanes x 2)"}
     roofline = {"bound": "hbm", "kernel": f"k_kick<4,3,float,FUND>" if dom == "kick" else "k_drift<3,float>",
                 "achieved": round(achieved, 1), "peak": hbm, "unit": "GB/s", "frac": round(achieved / hbm, 4),
                 "peak_source": peak_kind, "traffic": traffic,
@@ -254,7 +268,8 @@ def run_ours(a, dist):
                 "share_of_trajectory": round((share_kick if dom == "kick" else share_drift) / (r["ms"] / K), 3),
                 "fp64": {"kick_ms": round(res["fp64"]["kick_ms"], 5), "drift_ms": round(res["fp64"]["drift_ms"], 5),
                          "kick_GBps": round(V * ALG_BYTES["kick"]["fp64"] / (res["fp64"]["kick_ms"] / 1e3) / 1e9, 1)},
-                "fp32": {"kick_ms": round(r["kick_ms"], 5), "drift_ms": round(r["drift_ms"], 5)}}
+                "fp32": {"kick_ms": round(r["kick_ms"], 5), "drift_ms": round(r["drift_ms"], 5)},
+                "compute": compute}
 
     # ---- CPU baseline: the reference itself on this host's cores (rank 0, N=1) ----
     cpu = None
@@ -460,17 +475,14 @@ def run_extra(a, dist):
         for Lx in [int(x) for x in a.stage0_sizes.split(",")]:
             for prec in ("fp64", "fp32"):
                 rep = gh.GeneralRep(2, [12])
-                h = gh.GaugeHiggsHMC([Lx] * 4, rep, seed=1, precision=prec, beta=2.0, kappa=0.1, lam=0.5, nmd=20)
+                # |dH| grows with the volume: at 8^4 nmd = 20 gives |dH| ~ 10 and the chain sticks,
+                # so beyond 4^4 the step is halved per doubling of L (nmd = 20 L / 4), as the
+                # reference's scripts raise nmd where the force gets stiff
+                nmd = 20 * max(1, Lx // 4)
+                h = gh.GaugeHiggsHMC([Lx] * 4, rep, seed=1, precision=prec, beta=2.0, kappa=0.1, lam=0.5, nmd=nmd)
                 h.potential = gh.MultiInvariantPotential(gh.CasimirChannels(rep), f2i, 0.065)
-                # beyond 4^4 a hot start at nmd = 20 has |dH| >> 1 and the chain never leaves it;
-                # there the driver's GH_COLD start (identity links, phi = 1) is used
-                cold = Lx > 4
-                if cold:
-                    h.cold()
-                    h.phi_cold(1.0)
-                else:
-                    h.hot(0.8)
-                    h.phi_gaussian(12345, 0.3)
+                h.hot(0.8)
+                h.phi_gaussian(12345, 0.3)
                 v, rec = gpu_rate(h, 100 if Lx == 4 else 40, W=30)
                 cpu = None
                 if prec == "fp64" and Lx == 4 and ref is not None:
@@ -483,7 +495,7 @@ def run_extra(a, dist):
                            "sample": "3 trajectories after one"}
                     s.close()
                 out.append({"workload": f"SU(2) {{12}} (d=13) {Lx}^4, multi-invariant potential (13 channels, mu2=0.065), "
-                                        "beta=2.0 kappa=0.1, Omelyan nmd=20, " + ("cold start" if cold else "hot start"),
+                                        f"beta=2.0 kappa=0.1, Omelyan nmd={nmd}, hot start",
                             "precision": prec,
                             "value": round(v, 2), "unit": "trajectories/s",
                             "acceptance": float(rec["accepted"].mean()), "cpu_baseline": cpu})

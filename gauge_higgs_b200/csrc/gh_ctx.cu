@@ -443,7 +443,7 @@ int build_general(gh_ctx* ctx, const gh_rep_desc* r) {
       return rc;
     CK(cudaMemcpy(sptr, q.ptr.data(), q.ptr.size() * 4, cudaMemcpyHostToDevice));
     CK(cudaMemcpy(sc, q.c.data(), q.c.size() * 8, cudaMemcpyHostToDevice));
-    CK(cudaMemcpy(se, q.e.data(), q.e.size(), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(se, q.e.data(), q.e.size(), cudaMemcpyHostToDevice));   // N*N bytes per term, word-padded
     t.sp_ptr = sptr; t.sp_c = sc; t.sp_e = se;
   }
   return GH_OK;

@@ -564,10 +564,15 @@ __device__ void sympow_matrix(const GenTables& t, const Mat<N, C>& M, cx<double>
     for (int q = t.sp_ptr[e]; q < t.sp_ptr[e + 1]; ++q) {
       const double2 c = t.sp_c[q];
       cx<double> pr = mk<double>(c.x, c.y);
-      const unsigned char* ex = t.sp_e + (size_t)q * (N * N);
+      // exponents: N*N bytes per term, padded to whole 32-bit words
+      constexpr int EW = (N * N + 3) / 4;
+      const unsigned* ex = reinterpret_cast<const unsigned*>(t.sp_e) + (size_t)q * EW;
+      unsigned w[EW];
+#pragma unroll
+      for (int i = 0; i < EW; ++i) w[i] = __ldg(ex + i);
 #pragma unroll
       for (int ij = 0; ij < N * N; ++ij) {
-        const int k = ex[ij];
+        const int k = (w[ij >> 2] >> (8 * (ij & 3))) & 0xFF;
         if (k) pr = mul(pr, Pw[ij * (n + 1) + k]);
       }
       acc = add(acc, pr);
@@ -646,14 +651,18 @@ __global__ void __launch_bounds__(GEN_WARPS * 32) k_gen_links(const GenArgs a) {
   }
   if (sp) {
     sympow_matrix<N, C>(a.t, M, Dm, Pw, lane);
-    for (int k = lane; k < d; k += 32) {
-      cx<double> f = zero<double>(), b = zero<double>();
-      for (int l = 0; l < d; ++l) {
-        f = cfma(f, Dm[k * d + l], mk<double>((double)py[l].re, (double)py[l].im));
-        b = cfma_cj(b, Dm[l * d + k], mk<double>((double)px[l].re, (double)px[l].im));
+    // psi_f = D phi_y on lanes 0..d-1, psi_b = D^dag phi_x on the next d lanes
+    const int nv = a.mode == 1 ? d : 2 * d;
+    for (int t = lane; t < nv; t += 32) {
+      cx<double> acc = zero<double>();
+      if (t < d) {
+        for (int l = 0; l < d; ++l) acc = cfma(acc, Dm[t * d + l], mk<double>((double)py[l].re, (double)py[l].im));
+        pf[t] = mk<C>((C)acc.re, (C)acc.im);
+      } else {
+        const int k = t - d;
+        for (int l = 0; l < d; ++l) acc = cfma_cj(acc, Dm[l * d + k], mk<double>((double)px[l].re, (double)px[l].im));
+        pb[k] = mk<C>((C)acc.re, (C)acc.im);
       }
-      pf[k] = mk<C>((C)f.re, (C)f.im);
-      pb[k] = mk<C>((C)b.re, (C)b.im);
     }
     __syncwarp();
   } else {

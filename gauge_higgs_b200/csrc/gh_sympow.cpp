@@ -151,6 +151,7 @@ bool build(int N, int n, int d, long dimT, const double* W, long max_terms, Term
         out.c.push_back(c.real());
         out.c.push_back(c.imag());
         out.e.insert(out.e.end(), K.begin(), K.end());
+        out.e.resize(out.e.size() + (4 - (N * N) % 4) % 4, 0);   // whole 32-bit words per term
       }
       out.ptr[(size_t)k * d + l + 1] = (int)(out.c.size() / 2);
     }
@@ -182,7 +183,7 @@ void eval(const Terms& t, const double* Uin, double* Dout) {
     for (int q = t.ptr[e]; q < t.ptr[e + 1]; ++q) {
       cd pr(t.c[2 * (size_t)q], t.c[2 * (size_t)q + 1]);
       for (int ij = 0; ij < N * N; ++ij) {
-        const int k = t.e[(size_t)q * N * N + ij];
+        const int k = t.e[(size_t)q * ((N * N + 3) / 4 * 4) + ij];
         if (k) pr *= P[(size_t)ij * (n + 1) + k];
       }
       s += pr;

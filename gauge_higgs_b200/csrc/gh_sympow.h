@@ -23,7 +23,7 @@ struct Terms {
   int N = 0, n = 0, d = 0;
   std::vector<int> ptr;            // d*d + 1: terms of entry k*d + l
   std::vector<double> c;           // 2 per term: complex coefficient
-  std::vector<unsigned char> e;    // N*N per term: exponents K_ij (row-major)
+  std::vector<unsigned char> e;    // per term: exponents K_ij (row-major), N*N bytes padded to a multiple of 4
 };
 
 // Builds the term list when W ([d][dimT] complex, slot 0 the most significant base-N
