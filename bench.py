@@ -229,15 +229,21 @@ def run_ours(a, dist):
         h.trajectory_host(Uc, pc)
     torch.cuda.synchronize()
     dist.barrier()
+    n_acc = 0
     t0 = time.perf_counter()
     for _ in range(Ke):
-        h.trajectory_host(Uc, pc)
+        n_acc += int(h.trajectory_host(Uc, pc).accepted)
     torch.cuda.synchronize()
     e2e_s = dist.max(time.perf_counter() - t0)
+    # U and phi come back only after an accepted trajectory (a rejected one leaves the
+    # host fields as they were passed in); the record (56 B) and the lattice's descriptor with
+    # its trajectory counter (160 B) always
+    rec_bytes = 56 + 160
     e2e = {"value": dist.world * Ke / e2e_s, "unit": "trajectories/s",
            "h2d_bytes_per_step": int(U_host.nbytes + phi_host.nbytes),
-           "d2h_bytes_per_step": int(U_host.nbytes + phi_host.nbytes + 40), "steps": Ke,
-           "api": "gh_trajectory_host (pinned host U, phi in; U, phi, record out)"}
+           "d2h_bytes_per_step": int(round(n_acc / Ke * (U_host.nbytes + phi_host.nbytes))) + rec_bytes,
+           "steps": Ke, "accepted": n_acc,
+           "api": "gh_trajectory_host (pinned host U, phi in; record, and U, phi when accepted, out)"}
 
     # ---- roofline of the dominant kernel (FP32-MD path) ----
     hbm, peak_kind = peaks()

@@ -1187,20 +1187,22 @@ int gh_trajectory_host(gh_ctx* ctx, double* U, double* phi, gh_traj_record* rec)
   if (U && (rc = gh_set_links(ctx, 0, U))) return rc;
   if (phi && ctx->scalar && (rc = gh_set_phi(ctx, 0, phi))) return rc;
   if ((rc = run_traj(ctx))) return rc;
-  if (U && (rc = gh_get_links(ctx, 0, U))) return rc;
-  if (phi && ctx->scalar && (rc = gh_get_phi(ctx, 0, phi))) return rc;
+  // the record first: a rejected trajectory restores the state that was passed in, so
+  // the fields are only copied back when the trajectory was accepted
+  LatDev L;
+  TrajRec r;
+  CK(cudaMemcpyAsync(&L, ctx->b.lats, sizeof(L), cudaMemcpyDeviceToHost, ctx->st));
+  CK(cudaStreamSynchronize(ctx->st));
+  const int slot = (int)((L.traj - 1) % (unsigned long long)ctx->b.hist_cap);
+  CK(cudaMemcpy(&r, ctx->b.hist + slot, sizeof(r), cudaMemcpyDeviceToHost));
+  if (r.accepted) {
+    if (U && (rc = gh_get_links(ctx, 0, U))) return rc;
+    if (phi && ctx->scalar && (rc = gh_get_phi(ctx, 0, phi))) return rc;
+  }
   if (rec) {
-    LatDev L;
-    TrajRec r;
-    CK(cudaMemcpyAsync(&L, ctx->b.lats, sizeof(L), cudaMemcpyDeviceToHost, ctx->st));
-    CK(cudaStreamSynchronize(ctx->st));
-    const int slot = (int)((L.traj - 1) % (unsigned long long)ctx->b.hist_cap);
-    CK(cudaMemcpy(&r, ctx->b.hist + slot, sizeof(r), cudaMemcpyDeviceToHost));
     rec->dH = r.dH; rec->accepted = r.accepted; rec->traj = r.traj; rec->plaquette = r.plaq; rec->L_phi = r.L_phi; rec->L_link = r.L_link;
     rec->kappa = r.kappa;
     rec->beta = r.beta;
-  } else {
-    CK(cudaStreamSynchronize(ctx->st));
   }
   return GH_OK;
 }

@@ -181,7 +181,10 @@ int gh_enqueue_trajectories(gh_ctx* ctx, int ntraj);
 int gh_read_records(gh_ctx* ctx, int ntraj, gh_traj_record* records);
 /* Host-resident fields (single lattice): upload U and phi, run one trajectory,
  * download U, phi and the record.  The drop-in for a driver that keeps the
- * fields in host memory like the reference's GaugeField / CVecField. */
+ * fields in host memory like the reference's GaugeField / CVecField.  A rejected
+ * trajectory restores the state that was passed in, so U and phi are then left
+ * untouched (in FP32-MD mode they keep the caller's FP64 values rather than their
+ * FP32 roundings, which the next upload reproduces). */
 int gh_trajectory_host(gh_ctx* ctx, double* U, double* phi, gh_traj_record* rec);
 /* ---- kick tiles and the autotuner ----
  * The kick kernel gives each 128-thread block a 4-D tile of sites (power-of-two

@@ -497,3 +497,33 @@ def test_nonfinite_hamiltonian_is_rejected_and_counted(precision):
     assert np.all(np.isfinite(rec["dH"]))
     assert h.traj_counts(0)[2] == 1
     h.close()
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_trajectory_host_matches_device_chain(precision):
+    """gh_trajectory_host (fields in host memory, uploaded and downloaded every
+    trajectory; not downloaded after a rejection, which restores the uploaded state)
+    against the same chain kept on the device: identical records, identical fields
+    (FP32-MD: identical after rounding to FP32)."""
+    import gauge_higgs_b200 as gh
+    hs = []
+    for _ in range(2):
+        h = gh.GaugeHiggsHMC([4, 4, 4, 4], gh.FundamentalRep(3), seed=11, precision=precision, beta=5.7, kappa=0.1,
+                             lam=0.5, nmd=4)
+        h.hot(0.8)
+        h.phi_gaussian(12345, 0.3)
+        hs.append(h)
+    hA, hB = hs
+    U = np.ascontiguousarray(hA.U)
+    phi = np.ascontiguousarray(hA.phi)
+    recs = [hA.trajectory_host(U, phi) for _ in range(12)]
+    rB = hB.run(12)[:, 0]
+    assert [int(r.accepted) for r in recs] == [int(x) for x in rB["accepted"]]
+    assert np.array_equal(np.array([r.dH for r in recs]), rB["dH"])
+    if precision == "fp64":
+        assert np.array_equal(U, hB.U) and np.array_equal(phi, hB.phi)
+    else:
+        assert np.array_equal(U.astype(np.complex64), hB.U.astype(np.complex64))
+        assert np.array_equal(phi.astype(np.complex64), hB.phi.astype(np.complex64))
+    hA.close()
+    hB.close()
