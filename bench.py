@@ -522,7 +522,7 @@ def run_extra(a, dist):
         for k in kappas:
             for b in betas:
                 tiers.setdefault(nmd_for(k), []).append((b, k))
-        for prec in ("fp64", "fp32"):
+        for frozen, prec in ((False, "fp64"), (False, "fp32"), (True, "fp64")):
             K, total_s, acc = 20, 0.0, []
             for nmd, pts in sorted(tiers.items()):
                 rep = gh.GeneralRep(2, [12])
@@ -532,6 +532,9 @@ def run_extra(a, dist):
                 ens.potential = gh.MultiInvariantPotential(gh.CasimirChannels(rep), f2i, 0.065)
                 ens.hot(0.8)
                 ens.phi_gaussian(12345, 0.3)
+                if frozen:                  # the scan under GH_FROZEN: |phi_x| = 1
+                    ens.frozen_phi = True
+                    ens.normalize_phi()
                 v, rec = gpu_rate(ens, K, W=20)
                 total_s += K / v
                 acc.append(float(rec["accepted"].mean()))
@@ -544,6 +547,7 @@ def run_extra(a, dist):
                     b, k = pts[len(pts) // 2]
                     s = RefSession(ref, 4, 2, [2] * 4, "12", b, k, 0.5, nmd, 1.0, 1, OMELYAN, 0.8, 0.3)
                     s.set_multi(f2i, 0.065)
+                    s.set_frozen(frozen)
                     s.run(1)
                     t0 = time.perf_counter()
                     s.run(3)
@@ -554,7 +558,8 @@ def run_extra(a, dist):
                        "sample": "3 trajectories of one point per nmd tier, one thread; scaled to all 99 points "
                                  f"run {cores} at a time, as the script's JOBS=nproc"}
             out.append({"workload": "2I phase scan: SU(2) {12} 2^4, multi-invariant potential, beta 1.0..3.0 x kappa "
-                                    "0.0..1.0 (99 points), Omelyan nmd 16..68 by kappa, one ensemble per nmd tier",
+                                    "0.0..1.0 (99 points), Omelyan nmd 16..68 by kappa, one ensemble per nmd tier"
+                                    + (", frozen |phi| = 1 (GH_FROZEN)" if frozen else ""),
                         "precision": prec, "value": round(99 * K / total_s, 1),
                         "unit": "point trajectories/s", "acceptance_by_tier": [round(x, 3) for x in acc],
                         "cpu_baseline": cpu})

@@ -426,6 +426,7 @@ class Reference:
                                          C.c_int, C.c_double, _u64, C.c_int, C.c_double, C.c_double]
         L.ref_session_run.argtypes = [C.c_void_p, C.c_int, _dp]
         L.ref_session_set_multi.argtypes = [C.c_void_p, _dp, C.c_int, C.c_double]
+        L.ref_session_set_frozen.argtypes = [C.c_void_p, C.c_int]
         L.ref_session_acceptance.restype = C.c_double
         L.ref_session_acceptance.argtypes = [C.c_void_p]
         L.ref_session_destroy.argtypes = [C.c_void_p]
@@ -675,6 +676,11 @@ class RefSession:
         rc = self.lib.ref_session_set_multi(self.h, _d(f), len(f), mu2)
         if rc:
             raise RuntimeError(f"ref_session_set_multi rc={rc}")
+
+    def set_frozen(self, on=True):
+        """|phi_x| = 1 (GaugeHiggsHMC::frozen_phi) and the fields normalised, as the
+        driver does under GH_FROZEN (src/hmc_higgs_multi.cpp:81-82,90)."""
+        self.lib.ref_session_set_frozen(self.h, int(bool(on)))
 
     def acceptance(self):
         return self.lib.ref_session_acceptance(self.h)

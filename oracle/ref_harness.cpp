@@ -370,6 +370,7 @@ struct RefSession {
   virtual int run(int ntraj, double* series) = 0;   // series: [ntraj][5] as ref_run
   virtual double acceptance() = 0;
   virtual int set_multi(const double* f, int nf, double mu2) = 0;   // nf must equal the channel count
+  virtual void set_frozen(int on) = 0;                               // |phi_x| = 1, as GH_FROZEN
 };
 template <int DD, int NN>
 struct RefSessionT : RefSession {
@@ -398,6 +399,11 @@ struct RefSessionT : RefSession {
     h.potential = pot.get();
     return 0;
   }
+  // the driver's GH_FROZEN set-up (src/hmc_higgs_multi.cpp:81-82,90)
+  void set_frozen(int on) override {
+    h.frozen_phi = on != 0;
+    if (on) h.normalize_phi();
+  }
 };
 
 extern "C" {
@@ -417,6 +423,7 @@ int ref_session_run(void* s, int ntraj, double* series) { return s ? static_cast
 int ref_session_set_multi(void* s, const double* f, int nf, double mu2) {
   return s ? static_cast<RefSession*>(s)->set_multi(f, nf, mu2) : -1;
 }
+void ref_session_set_frozen(void* s, int on) { if (s) static_cast<RefSession*>(s)->set_frozen(on); }
 double ref_session_acceptance(void* s) { return s ? static_cast<RefSession*>(s)->acceptance() : 0.0; }
 void ref_session_destroy(void* s) { delete static_cast<RefSession*>(s); }
 
