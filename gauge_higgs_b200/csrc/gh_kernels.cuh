@@ -101,21 +101,25 @@ template <typename C, typename R> __device__ __forceinline__ void stc(R* p, long
   v.y = (R)z.im;
   reinterpret_cast<typename V2<R>::t*>(p)[i] = v;
 }
+// Sites are never negative: the 32-site block and lane come from a shift and a mask
+// (a signed division by 32 costs the rounding fix-up on every address).
+__device__ __forceinline__ long long site_blk(int s) { return (long long)((unsigned)s >> 5); }
+__device__ __forceinline__ int site_lane(int s) { return (int)((unsigned)s & (ULANE - 1)); }
 // Element index of component c of link (mu, s); component c + k sits k * ULANE further on.
 __device__ __forceinline__ long long u_index(const LatDev& L, int nn, int mu, int c, int s) {
-  return L.u_off + (long long)mu * nn * L.Vp + ((long long)(s / ULANE) * nn + c) * ULANE + (s % ULANE);
+  return L.u_off + (long long)mu * nn * L.Vp + (site_blk(s) * nn + c) * ULANE + site_lane(s);
 }
 // Momenta P: [mu][site/32][a][site%32] (ng components, direction planes of ng * Vp)
 __device__ __forceinline__ long long p_index(const LatDev& L, int ng, int mu, int g, int s) {
-  return L.p_off + (long long)mu * ng * L.Vp + ((long long)(s / ULANE) * ng + g) * ULANE + (s % ULANE);
+  return L.p_off + (long long)mu * ng * L.Vp + (site_blk(s) * ng + g) * ULANE + site_lane(s);
 }
 // Scalar fields phi, pi: [site/32][k][site%32] (d components)
 __device__ __forceinline__ long long f_index(const LatDev& L, int d, int k, int s) {
-  return L.f_off + ((long long)(s / ULANE) * d + k) * ULANE + (s % ULANE);
+  return L.f_off + (site_blk(s) * d + k) * ULANE + site_lane(s);
 }
 // General-irrep scratch psi_f, psi_b: [mu][site/32][k][site%32]
 __device__ __forceinline__ long long g_index(const LatDev& L, int d, int mu, int k, int s) {
-  return L.g_off + (long long)mu * d * L.Vp + ((long long)(s / ULANE) * d + k) * ULANE + (s % ULANE);
+  return L.g_off + (long long)mu * d * L.Vp + (site_blk(s) * d + k) * ULANE + site_lane(s);
 }
 template <int N, typename C, typename R>
 __device__ __forceinline__ Mat<N, C> ld_link(const R* __restrict__ U, const LatDev& L, int mu, int s) {
