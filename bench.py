@@ -161,7 +161,10 @@ def run_ours(a, dist):
         h.set_stream(stream.cuda_stream)
         h.hot(WL["hot_sigma"])
         h.phi_gaussian(12345, WL["phi_sigma"])
-        h.autotune(reps=3)          # kick tile shape chosen by timing (results do not depend on it)
+        if a.kick_tile:             # a fixed tile (profiling runs: timing-based choices under a profiler are not representative)
+            h.set_tile([int(x) for x in a.kick_tile.split(",")])
+        else:
+            h.autotune(reps=3)      # kick tile shape chosen by timing (results do not depend on it)
         return h
 
     def timed(h, K, W, sampler=None):
@@ -633,6 +636,7 @@ def main():
     ap.add_argument("--cpu-traj", type=int, default=3)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--stage0-sizes", default="4,8", help="lattice extents of --workload stage0 (comma list)")
+    ap.add_argument("--kick-tile", default="", help="fixed kick tile (e.g. 16,2,2,2) instead of the timed choice")
     ap.add_argument("--validate-traj", type=int, default=2000)
     ap.add_argument("--validate-therm", type=int, default=200)
     ap.add_argument("--workload", default="c2", choices=["c2", "c1", "c3", "c4", "big", "stage0", "scan", "validate", "all"],
