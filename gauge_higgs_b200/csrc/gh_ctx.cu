@@ -1043,8 +1043,10 @@ int gh_autotune(gh_ctx* ctx, int reps, double* best_ms) {
 }
 
 // Multi-invariant onsite potential (src/action/scalar_invariants.hpp:190-206): the
-// channel superoperator is built on the host (gh_potential.cpp) and copied to the
-// device in both precisions; the kick's site items and the measure kernel apply it.
+// channel superoperator is built on the host (gh_potential.cpp) and its nonzero entries
+// are copied to the device (values in both precisions).  The kick's site items and the
+// measure kernel apply it for the fundamental and adjoint; for general irreps the link
+// kernel computes w = A(M) phi once per site and both read that.
 int gh_set_potential_multi(gh_ctx* ctx, int n_channels, const double* f, double mu2) {
   if (!ctx) return fail(nullptr, GH_ERR_ARG, "null context");
   if (!ctx->scalar) return fail(ctx, GH_ERR_STATE, "no scalar field in a pure-gauge context");
