@@ -439,11 +439,11 @@ int build_general(gh_ctx* ctx, const gh_rep_desc* r) {
     int* sptr;
     double2* sc;
     unsigned char* se;
-    if ((rc = dalloc(ctx, &sptr, q.ptr.size())) || (rc = dalloc(ctx, &sc, q.c.size() / 2)) || (rc = dalloc(ctx, &se, q.e.size())))
+    if ((rc = dalloc(ctx, &sptr, q.ptr.size())) || (rc = dalloc(ctx, &sc, q.c.size() / 2)) || (rc = dalloc(ctx, &se, q.off.size())))
       return rc;
     CK(cudaMemcpy(sptr, q.ptr.data(), q.ptr.size() * 4, cudaMemcpyHostToDevice));
     CK(cudaMemcpy(sc, q.c.data(), q.c.size() * 8, cudaMemcpyHostToDevice));
-    CK(cudaMemcpy(se, q.e.data(), q.e.size(), cudaMemcpyHostToDevice));   // N*N bytes per term, word-padded
+    CK(cudaMemcpy(se, q.off.data(), q.off.size(), cudaMemcpyHostToDevice));   // power-table offsets, word-padded
     t.sp_ptr = sptr; t.sp_c = sc; t.sp_e = se;
   }
   return GH_OK;

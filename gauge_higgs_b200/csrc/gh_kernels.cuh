@@ -549,8 +549,9 @@ __device__ void gen_apply(const GenTables& t, const Mat<N, C>& M, bool dag, cons
 
 // D(U) of a single-row irrep from its term list, FP64, one warp:
 //   D[k][l] = sum_terms c prod_ij U_ij^K_ij
-// with the powers U_ij^p (p = 0..n) tabulated first.  Dm: d*d, Pw: N*N*(n+1) entries
-// of this warp's shared memory.
+// with the powers U_ij^p (p = 0..n) tabulated first (entry ij*(n+1) + p) and each term
+// given by its offsets into that table.  Dm: d*d, Pw: N*N*(n+1) entries of this warp's
+// shared memory.
 template <int N, typename C>
 __device__ void sympow_matrix(const GenTables& t, const Mat<N, C>& M, cx<double>* Dm, cx<double>* Pw, int lane) {
   const int n = t.n, d = t.d;
@@ -568,16 +569,24 @@ __device__ void sympow_matrix(const GenTables& t, const Mat<N, C>& M, cx<double>
     for (int q = t.sp_ptr[e]; q < t.sp_ptr[e + 1]; ++q) {
       const double2 c = t.sp_c[q];
       cx<double> pr = mk<double>(c.x, c.y);
-      // exponents: N*N bytes per term, padded to whole 32-bit words
+      // offsets into the power table, N*N bytes per term in whole 32-bit words: SU(2)
+      // multiplies all four factors (an exponent 0 points at a 1), larger N the nonzero
+      // factors up to the first 0xFF
       constexpr int EW = (N * N + 3) / 4;
       const unsigned* ex = reinterpret_cast<const unsigned*>(t.sp_e) + (size_t)q * EW;
       unsigned w[EW];
 #pragma unroll
       for (int i = 0; i < EW; ++i) w[i] = __ldg(ex + i);
+      if constexpr (N == 2) {
 #pragma unroll
-      for (int ij = 0; ij < N * N; ++ij) {
-        const int k = (w[ij >> 2] >> (8 * (ij & 3))) & 0xFF;
-        if (k) pr = mul(pr, Pw[ij * (n + 1) + k]);
+        for (int f = 0; f < 4; ++f) pr = mul(pr, Pw[(w[0] >> (8 * f)) & 0xFF]);
+      } else {
+#pragma unroll
+        for (int f = 0; f < N * N; ++f) {
+          const unsigned o = (w[f >> 2] >> (8 * (f & 3))) & 0xFF;
+          if (o == 0xFF) break;
+          pr = mul(pr, Pw[o]);
+        }
       }
       acc = add(acc, pr);
     }

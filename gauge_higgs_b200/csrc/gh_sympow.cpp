@@ -96,6 +96,7 @@ void su_link(int N, int which, cd* U) {
 bool build(int N, int n, int d, long dimT, const double* W, long max_terms, Terms& out, std::string* why) {
   auto no = [&](const char* m) { if (why) *why = m; return false; };
   if (N < 2 || n < 1 || d < 1 || dimT < 1 || !W) return no("bad arguments");
+  if (N * N * (n + 1) > 255) return no("power table too large for byte offsets");
   long pw = 1;
   for (int k = 0; k < n; ++k) pw *= N;
   if (pw != dimT) return no("dimT != N^n");
@@ -152,6 +153,10 @@ bool build(int N, int n, int d, long dimT, const double* W, long max_terms, Term
         out.c.push_back(c.imag());
         out.e.insert(out.e.end(), K.begin(), K.end());
         out.e.resize(out.e.size() + (4 - (N * N) % 4) % 4, 0);   // whole 32-bit words per term
+        const size_t o0 = out.off.size();
+        for (int ij = 0; ij < N * N; ++ij)
+          if (N == 2 || K[ij] > 0) out.off.push_back((unsigned char)(ij * (n + 1) + K[ij]));
+        out.off.resize(o0 + (N * N + 3) / 4 * 4, 0xFF);
       }
       out.ptr[(size_t)k * d + l + 1] = (int)(out.c.size() / 2);
     }

@@ -24,6 +24,10 @@ struct Terms {
   std::vector<int> ptr;            // d*d + 1: terms of entry k*d + l
   std::vector<double> c;           // 2 per term: complex coefficient
   std::vector<unsigned char> e;    // per term: exponents K_ij (row-major), N*N bytes padded to a multiple of 4
+  // per term, for the device: offsets ij*(n+1) + K_ij into the table of powers U_ij^p, as
+  // bytes in whole 32-bit words.  N = 2: all four factors (an exponent 0 points at the
+  // table's 1); N > 2: the factors with K_ij > 0, in ij order, then 0xFF.
+  std::vector<unsigned char> off;
 };
 
 // Builds the term list when W ([d][dimT] complex, slot 0 the most significant base-N
