@@ -431,8 +431,9 @@ def run_extra(a, dist):
                         "cpu_baseline": cpu_rate(4, 2, [6] * 4, "fund", 2.3, 0.2, 0.5, 20, LEAPFROG, 60) if prec == "fp64" else None})
             h.close()
     if wl in ("c3", "all"):
-        for spec, rows, real in (("sextet {2}", [2], False), ("octet {2,1}:real", [2, 1], True),
-                                 ("27-plet {4,2}:real", [4, 2], True)):
+        c3 = {"sextet": ("sextet {2}", [2], False), "octet": ("octet {2,1}:real", [2, 1], True),
+              "27plet": ("27-plet {4,2}:real", [4, 2], True)}
+        for spec, rows, real in (c3[k] for k in a.c3_reps.split(",")):
             for prec in ("fp64", "fp32"):
                 rep = gh.GeneralRep(3, rows, real=real)
                 h = gh.GaugeHiggsHMC([12] * 4, rep, seed=1, precision=prec, beta=5.7, kappa=0.1, lam=0.5, nmd=20)
@@ -636,6 +637,7 @@ def main():
     ap.add_argument("--cpu-traj", type=int, default=3)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--stage0-sizes", default="4,8", help="lattice extents of --workload stage0 (comma list)")
+    ap.add_argument("--c3-reps", default="sextet,octet,27plet", help="irreps of --workload c3 (comma list)")
     ap.add_argument("--kick-tile", default="", help="fixed kick tile (e.g. 16,2,2,2) instead of the timed choice")
     ap.add_argument("--validate-traj", type=int, default=2000)
     ap.add_argument("--validate-therm", type=int, default=200)

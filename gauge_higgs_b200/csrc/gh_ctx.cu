@@ -414,6 +414,8 @@ int build_general(gh_ctx* ctx, const gh_rep_desc* r) {
   t.d = d; t.n = r->n_boxes; t.dimT = (int)dimT; t.ng = ng;
   t.powN[0] = 1;
   for (int k = 1; k < 18; ++k) t.powN[k] = (k <= r->n_boxes) ? t.powN[k - 1] * N : 0;
+  for (int k = 0; k < 18; ++k)
+    t.pmag[k] = (k >= 1 && t.powN[k] > 0) ? (unsigned)(((1ULL << 32) + (unsigned long long)t.powN[k] - 1) / t.powN[k]) : 0u;
   int *p1, *p2, *p3, *p4, *p5, *p6;
   double2 *v1, *v2, *v3;
   int rc;

@@ -73,6 +73,9 @@ struct Work { int lat, mu, s0, n; };
 struct GenTables {                 // general irrep (src/rep/rep_general.hpp), sparse
   int d, n, dimT, ng;
   int powN[18];
+  // division by powN[k] as a multiply-high: q = umulhi(f, pmag[k]) for k >= 1 (exact for
+  // f * powN[k] < 2^32, which N^n <= 200000 guarantees); powN[0] = 1 needs none
+  unsigned pmag[18];
   const int* wt_ptr; const int* wt_l; const double2* wt_v;   // lift: CSR over tensor index
   const int* w_ptr;  const int* w_i;  const double2* w_v;    // project: CSR over basis vector
   const int* t_ptr;  const int* t_j;  const double2* t_v;    // T^a_R: CSR over (a, row)
@@ -519,9 +522,12 @@ __device__ void gen_apply(const GenTables& t, const Mat<N, C>& M, bool dag, cons
   // slot applies: fibre f of slot sl holds the N entries base + j*blk
   const int nf = t.dimT / N;
   for (int sl = 0; sl < t.n; ++sl) {
-    const int blk = t.powN[t.n - 1 - sl];
+    const int k = t.n - 1 - sl;
+    const int blk = t.powN[k];
+    const unsigned mag = t.pmag[k];
     for (int f = lane; f < nf; f += 32) {
-      const int base = (f / blk) * blk * N + (f % blk);
+      const int q = (k == 0) ? f : (int)__umulhi((unsigned)f, mag);
+      const int base = q * blk * (N - 1) + f;      // (f / blk) * blk * N + f % blk
       cx<C> v[N];
 #pragma unroll
       for (int j = 0; j < N; ++j) v[j] = buf[base + j * blk];
