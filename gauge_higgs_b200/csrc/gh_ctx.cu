@@ -92,6 +92,10 @@ int fail(gh_ctx* c, int code, const std::string& m) {
   if (c) c->err = m; else g_err = m;
   return code;
 }
+// Copies and fills outside the trajectory run on the context's stream (cudaMemcpyAsync /
+// cudaMemsetAsync, a synchronise after every read back): that stream is non-blocking, so
+// a plain cudaMemcpy on the legacy default stream is not ordered with its kernels, and
+// one from pageable memory may return before its transfer has landed.
 #define CK(call)                                                                          \
   do {                                                                                    \
     cudaError_t e_ = (call);                                                              \
@@ -105,7 +109,7 @@ int dalloc(gh_ctx* ctx, T** p, size_t n) {
   const size_t bytes = std::max<size_t>(n, 1) * sizeof(T);
   cudaError_t e = cudaMalloc(&q, bytes);
   if (e != cudaSuccess) return fail(ctx, GH_ERR_CUDA, std::string("cudaMalloc: ") + cudaGetErrorString(e));
-  cudaMemset(q, 0, bytes);
+  cudaMemsetAsync(q, 0, bytes, ctx->st);
   ctx->allocs.push_back(q);
   ctx->bytes += bytes;
   *p = (T*)q;
@@ -348,7 +352,7 @@ int upload_kick_items(gh_ctx* ctx, const std::vector<Work>& items, int nlinks, i
     CK(cudaMalloc(&ctx->wk_dev, sizeof(Work) * items.size()));
     ctx->wk_cap = items.size();
   }
-  CK(cudaMemcpy(ctx->wk_dev, items.data(), sizeof(Work) * items.size(), cudaMemcpyHostToDevice));
+  CK(cudaMemcpyAsync(ctx->wk_dev, items.data(), sizeof(Work) * items.size(), cudaMemcpyHostToDevice, ctx->st));
   ctx->b.w_kick = ctx->wk_dev;
   ctx->b.nwk_links = nlinks;
   ctx->b.nwk_sites = nsites;
@@ -357,7 +361,7 @@ int upload_kick_items(gh_ctx* ctx, const std::vector<Work>& items, int nlinks, i
 
 int push_tiles(gh_ctx* ctx) {
   for (int l = 0; l < ctx->nlat; ++l)
-    CK(cudaMemcpy((char*)(ctx->b.lats + l) + offsetof(LatDev, lt), ctx->lat_h[l].lt, sizeof(int) * 4, cudaMemcpyHostToDevice));
+    CK(cudaMemcpyAsync((char*)(ctx->b.lats + l) + offsetof(LatDev, lt), ctx->lat_h[l].lt, sizeof(int) * 4, cudaMemcpyHostToDevice, ctx->st));
   return GH_OK;
 }
 
@@ -423,15 +427,15 @@ int build_general(gh_ctx* ctx, const gh_rep_desc* r) {
       (rc = dalloc(ctx, &p3, w_ptr.size())) || (rc = dalloc(ctx, &p4, w_i.size())) || (rc = dalloc(ctx, &v2, w_v.size())) ||
       (rc = dalloc(ctx, &p5, t_ptr.size())) || (rc = dalloc(ctx, &p6, t_j.size())) || (rc = dalloc(ctx, &v3, t_v.size())))
     return rc;
-  CK(cudaMemcpy(p1, wt_ptr.data(), wt_ptr.size() * 4, cudaMemcpyHostToDevice));
-  if (!wt_l.empty()) CK(cudaMemcpy(p2, wt_l.data(), wt_l.size() * 4, cudaMemcpyHostToDevice));
-  if (!wt_v.empty()) CK(cudaMemcpy(v1, wt_v.data(), wt_v.size() * 16, cudaMemcpyHostToDevice));
-  CK(cudaMemcpy(p3, w_ptr.data(), w_ptr.size() * 4, cudaMemcpyHostToDevice));
-  if (!w_i.empty()) CK(cudaMemcpy(p4, w_i.data(), w_i.size() * 4, cudaMemcpyHostToDevice));
-  if (!w_v.empty()) CK(cudaMemcpy(v2, w_v.data(), w_v.size() * 16, cudaMemcpyHostToDevice));
-  CK(cudaMemcpy(p5, t_ptr.data(), t_ptr.size() * 4, cudaMemcpyHostToDevice));
-  if (!t_j.empty()) CK(cudaMemcpy(p6, t_j.data(), t_j.size() * 4, cudaMemcpyHostToDevice));
-  if (!t_v.empty()) CK(cudaMemcpy(v3, t_v.data(), t_v.size() * 16, cudaMemcpyHostToDevice));
+  CK(cudaMemcpyAsync(p1, wt_ptr.data(), wt_ptr.size() * 4, cudaMemcpyHostToDevice, ctx->st));
+  if (!wt_l.empty()) CK(cudaMemcpyAsync(p2, wt_l.data(), wt_l.size() * 4, cudaMemcpyHostToDevice, ctx->st));
+  if (!wt_v.empty()) CK(cudaMemcpyAsync(v1, wt_v.data(), wt_v.size() * 16, cudaMemcpyHostToDevice, ctx->st));
+  CK(cudaMemcpyAsync(p3, w_ptr.data(), w_ptr.size() * 4, cudaMemcpyHostToDevice, ctx->st));
+  if (!w_i.empty()) CK(cudaMemcpyAsync(p4, w_i.data(), w_i.size() * 4, cudaMemcpyHostToDevice, ctx->st));
+  if (!w_v.empty()) CK(cudaMemcpyAsync(v2, w_v.data(), w_v.size() * 16, cudaMemcpyHostToDevice, ctx->st));
+  CK(cudaMemcpyAsync(p5, t_ptr.data(), t_ptr.size() * 4, cudaMemcpyHostToDevice, ctx->st));
+  if (!t_j.empty()) CK(cudaMemcpyAsync(p6, t_j.data(), t_j.size() * 4, cudaMemcpyHostToDevice, ctx->st));
+  if (!t_v.empty()) CK(cudaMemcpyAsync(v3, t_v.data(), t_v.size() * 16, cudaMemcpyHostToDevice, ctx->st));
   t.wt_ptr = p1; t.wt_l = p2; t.wt_v = v1; t.w_ptr = p3; t.w_i = p4; t.w_v = v2; t.t_ptr = p5; t.t_j = p6; t.t_v = v3;
   t.sp_ptr = nullptr; t.sp_c = nullptr; t.sp_e = nullptr;
   t.warp_bytes = (int)ctx->gen_warp_bytes;
@@ -443,9 +447,9 @@ int build_general(gh_ctx* ctx, const gh_rep_desc* r) {
     unsigned char* se;
     if ((rc = dalloc(ctx, &sptr, q.ptr.size())) || (rc = dalloc(ctx, &sc, q.c.size() / 2)) || (rc = dalloc(ctx, &se, q.off.size())))
       return rc;
-    CK(cudaMemcpy(sptr, q.ptr.data(), q.ptr.size() * 4, cudaMemcpyHostToDevice));
-    CK(cudaMemcpy(sc, q.c.data(), q.c.size() * 8, cudaMemcpyHostToDevice));
-    CK(cudaMemcpy(se, q.off.data(), q.off.size(), cudaMemcpyHostToDevice));   // power-table offsets, word-padded
+    CK(cudaMemcpyAsync(sptr, q.ptr.data(), q.ptr.size() * 4, cudaMemcpyHostToDevice, ctx->st));
+    CK(cudaMemcpyAsync(sc, q.c.data(), q.c.size() * 8, cudaMemcpyHostToDevice, ctx->st));
+    CK(cudaMemcpyAsync(se, q.off.data(), q.off.size(), cudaMemcpyHostToDevice, ctx->st));   // power-table offsets, word-padded
     t.sp_ptr = sptr; t.sp_c = sc; t.sp_e = se;
   }
   return GH_OK;
@@ -602,10 +606,10 @@ int gh_ctx_create(int D, int N, int n_lat, const int* L, const gh_rep_desc* rep,
       (rc = dalloc(ctx, &ctx->fphibuf, (size_t)std::max<long long>(f, 1) * 2)))
     { g_err = ctx->err; return rc; }
   ctx->staging_elems = stage;
-  CK(cudaMemcpy(b.lats, ctx->lat_h.data(), sizeof(LatDev) * n_lat, cudaMemcpyHostToDevice));
-  CK(cudaMemcpy(b.w_all, wall.data(), sizeof(Work) * wall.size(), cudaMemcpyHostToDevice));
-  if (!wg.empty()) CK(cudaMemcpy(b.w_gen, wg.data(), sizeof(Work) * wg.size(), cudaMemcpyHostToDevice));
-  CK(cudaMemcpy(b.blk_first, blk_first.data(), sizeof(int) * blk_first.size(), cudaMemcpyHostToDevice));
+  CK(cudaMemcpyAsync(b.lats, ctx->lat_h.data(), sizeof(LatDev) * n_lat, cudaMemcpyHostToDevice, ctx->st));
+  CK(cudaMemcpyAsync(b.w_all, wall.data(), sizeof(Work) * wall.size(), cudaMemcpyHostToDevice, ctx->st));
+  if (!wg.empty()) CK(cudaMemcpyAsync(b.w_gen, wg.data(), sizeof(Work) * wg.size(), cudaMemcpyHostToDevice, ctx->st));
+  CK(cudaMemcpyAsync(b.blk_first, blk_first.data(), sizeof(int) * blk_first.size(), cudaMemcpyHostToDevice, ctx->st));
   if ((rc = rebuild_kick_table(ctx))) { g_err = ctx->err; return rc; }
   if (ctx->rep == REP_GEN) {
     const size_t sm = ctx->eng->gen_smem(b);
@@ -668,7 +672,7 @@ int gh_set_couplings(gh_ctx* ctx, int lat, double beta, double kappa, double lam
   for (int l = l0; l < l1; ++l) {
     double v[3] = {beta, kappa, lambda};
     ctx->lat_h[l].beta = beta; ctx->lat_h[l].kappa = kappa; ctx->lat_h[l].lambda = lambda;
-    CK(cudaMemcpy((char*)(ctx->b.lats + l) + offsetof(LatDev, beta), v, sizeof(v), cudaMemcpyHostToDevice));
+    CK(cudaMemcpyAsync((char*)(ctx->b.lats + l) + offsetof(LatDev, beta), v, sizeof(v), cudaMemcpyHostToDevice, ctx->st));
   }
   return GH_OK;
 }
@@ -678,7 +682,8 @@ int gh_get_couplings(gh_ctx* ctx, int lat, double* beta, double* kappa, double* 
   if (rc) return rc;
   LatDev L;
   CK(cudaStreamSynchronize(ctx->st));
-  CK(cudaMemcpy(&L, ctx->b.lats + lat, sizeof(L), cudaMemcpyDeviceToHost));
+  CK(cudaMemcpyAsync(&L, ctx->b.lats + lat, sizeof(L), cudaMemcpyDeviceToHost, ctx->st));
+  CK(cudaStreamSynchronize(ctx->st));
   if (beta) *beta = L.beta;
   if (kappa) *kappa = L.kappa;
   if (lambda) *lambda = L.lambda;
@@ -701,7 +706,7 @@ int gh_set_traj_count(gh_ctx* ctx, int lat, uint64_t traj_count, uint64_t accept
   const int l0 = lat < 0 ? 0 : lat, l1 = lat < 0 ? ctx->nlat : lat + 1;
   for (int l = l0; l < l1; ++l) {
     unsigned long long v[2] = {traj_count, accept_count};
-    CK(cudaMemcpy((char*)(ctx->b.lats + l) + offsetof(LatDev, traj), v, sizeof(v), cudaMemcpyHostToDevice));
+    CK(cudaMemcpyAsync((char*)(ctx->b.lats + l) + offsetof(LatDev, traj), v, sizeof(v), cudaMemcpyHostToDevice, ctx->st));
   }
   return GH_OK;
 }
@@ -711,7 +716,8 @@ int gh_get_traj_count(gh_ctx* ctx, int lat, uint64_t* traj_count, uint64_t* acce
   if (rc) return rc;
   LatDev L;
   CK(cudaStreamSynchronize(ctx->st));
-  CK(cudaMemcpy(&L, ctx->b.lats + lat, sizeof(L), cudaMemcpyDeviceToHost));
+  CK(cudaMemcpyAsync(&L, ctx->b.lats + lat, sizeof(L), cudaMemcpyDeviceToHost, ctx->st));
+  CK(cudaStreamSynchronize(ctx->st));
   if (traj_count) *traj_count = L.traj;
   if (accept_count) *accept_count = L.accepted;
   if (nonfinite_count) *nonfinite_count = L.nonfinite;
@@ -1085,11 +1091,11 @@ int gh_set_potential_multi(gh_ctx* ctx, int n_channels, const double* f, double 
   CK(cudaMalloc(&ctx->sa_ij, nz * sizeof(unsigned short)));
   CK(cudaMalloc(&ctx->sa_v64, nz * sizeof(double2)));
   CK(cudaMalloc(&ctx->sa_v32, nz * sizeof(float2)));
-  CK(cudaMemcpy(ctx->sa_ptr, ptr.data(), ptr.size() * sizeof(int), cudaMemcpyHostToDevice));
+  CK(cudaMemcpyAsync(ctx->sa_ptr, ptr.data(), ptr.size() * sizeof(int), cudaMemcpyHostToDevice, ctx->st));
   if (!ij.empty()) {
-    CK(cudaMemcpy(ctx->sa_ij, ij.data(), ij.size() * sizeof(unsigned short), cudaMemcpyHostToDevice));
-    CK(cudaMemcpy(ctx->sa_v64, v64.data(), v64.size() * sizeof(double2), cudaMemcpyHostToDevice));
-    CK(cudaMemcpy(ctx->sa_v32, v32.data(), v32.size() * sizeof(float2), cudaMemcpyHostToDevice));
+    CK(cudaMemcpyAsync(ctx->sa_ij, ij.data(), ij.size() * sizeof(unsigned short), cudaMemcpyHostToDevice, ctx->st));
+    CK(cudaMemcpyAsync(ctx->sa_v64, v64.data(), v64.size() * sizeof(double2), cudaMemcpyHostToDevice, ctx->st));
+    CK(cudaMemcpyAsync(ctx->sa_v32, v32.data(), v32.size() * sizeof(float2), cudaMemcpyHostToDevice, ctx->st));
   }
   ctx->b.sa64 = PotA{ctx->sa_ptr, ctx->sa_ij, ctx->sa_v64};
   ctx->b.sa32 = PotA{ctx->sa_ptr, ctx->sa_ij, ctx->sa_v32};
@@ -1198,7 +1204,8 @@ int gh_trajectory_host(gh_ctx* ctx, double* U, double* phi, gh_traj_record* rec)
   CK(cudaMemcpyAsync(&L, ctx->b.lats, sizeof(L), cudaMemcpyDeviceToHost, ctx->st));
   CK(cudaStreamSynchronize(ctx->st));
   const int slot = (int)((L.traj - 1) % (unsigned long long)ctx->b.hist_cap);
-  CK(cudaMemcpy(&r, ctx->b.hist + slot, sizeof(r), cudaMemcpyDeviceToHost));
+  CK(cudaMemcpyAsync(&r, ctx->b.hist + slot, sizeof(r), cudaMemcpyDeviceToHost, ctx->st));
+  CK(cudaStreamSynchronize(ctx->st));
   if (r.accepted) {
     if (U && (rc = gh_get_links(ctx, 0, U))) return rc;
     if (phi && ctx->scalar && (rc = gh_get_phi(ctx, 0, phi))) return rc;
@@ -1219,7 +1226,8 @@ int gh_temper_enable(gh_ctx* ctx, int mode, uint64_t swap_seed) {
   if (mode == 1 && !ctx->scalar) return fail(ctx, GH_ERR_STATE, "kappa tempering needs a scalar field");
   CK(cudaStreamSynchronize(ctx->st));
   std::vector<LatDev> L(ctx->nlat);
-  CK(cudaMemcpy(L.data(), ctx->b.lats, sizeof(LatDev) * ctx->nlat, cudaMemcpyDeviceToHost));
+  CK(cudaMemcpyAsync(L.data(), ctx->b.lats, sizeof(LatDev) * ctx->nlat, cudaMemcpyDeviceToHost, ctx->st));
+  CK(cudaStreamSynchronize(ctx->st));
   // group lattices by extents, order each group by kappa
   std::map<std::vector<int>, std::vector<int>> groups;
   for (int l = 0; l < ctx->nlat; ++l) groups[std::vector<int>(L[l].L, L[l].L + ctx->D)].push_back(l);
@@ -1245,10 +1253,10 @@ int gh_temper_enable(gh_ctx* ctx, int mode, uint64_t swap_seed) {
         (rc = dalloc(ctx, &ctx->t_stats, 2 * ctx->nlat + 1)) || (rc = dalloc(ctx, &ctx->t_pairmap, ctx->nlat)))
       return rc;
   }
-  CK(cudaMemcpy(ctx->t_order, order.data(), sizeof(int) * order.size(), cudaMemcpyHostToDevice));
-  CK(cudaMemcpy(ctx->t_groups, gb.data(), sizeof(int) * gb.size(), cudaMemcpyHostToDevice));
-  CK(cudaMemcpy(ctx->t_pairmap, pairmap.data(), sizeof(int) * pairmap.size(), cudaMemcpyHostToDevice));
-  CK(cudaMemset(ctx->t_stats, 0, sizeof(unsigned long long) * (2 * ctx->nlat + 1)));
+  CK(cudaMemcpyAsync(ctx->t_order, order.data(), sizeof(int) * order.size(), cudaMemcpyHostToDevice, ctx->st));
+  CK(cudaMemcpyAsync(ctx->t_groups, gb.data(), sizeof(int) * gb.size(), cudaMemcpyHostToDevice, ctx->st));
+  CK(cudaMemcpyAsync(ctx->t_pairmap, pairmap.data(), sizeof(int) * pairmap.size(), cudaMemcpyHostToDevice, ctx->st));
+  CK(cudaMemsetAsync(ctx->t_stats, 0, sizeof(unsigned long long) * (2 * ctx->nlat + 1), ctx->st));
   ctx->t_ngroups = (int)gb.size() - 1;
   ctx->temper = mode;
   ctx->swap_seed = swap_seed;
@@ -1269,7 +1277,8 @@ int gh_temper_stats(gh_ctx* ctx, uint64_t* attempts, uint64_t* accepts, double* 
   CK(cudaStreamSynchronize(ctx->st));
   if (ctx->t_stats) {
     std::vector<unsigned long long> s(2 * ctx->nlat + 1);
-    CK(cudaMemcpy(s.data(), ctx->t_stats, sizeof(unsigned long long) * s.size(), cudaMemcpyDeviceToHost));
+    CK(cudaMemcpyAsync(s.data(), ctx->t_stats, sizeof(unsigned long long) * s.size(), cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
     for (int k = 0; k < ctx->nlat - 1; ++k) {
       if (attempts) attempts[k] = s[k];
       if (accepts) accepts[k] = s[ctx->nlat + k];
@@ -1277,7 +1286,8 @@ int gh_temper_stats(gh_ctx* ctx, uint64_t* attempts, uint64_t* accepts, double* 
   }
   if (kappa_of_lat) {
     std::vector<LatDev> L(ctx->nlat);
-    CK(cudaMemcpy(L.data(), ctx->b.lats, sizeof(LatDev) * ctx->nlat, cudaMemcpyDeviceToHost));
+    CK(cudaMemcpyAsync(L.data(), ctx->b.lats, sizeof(LatDev) * ctx->nlat, cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
     for (int l = 0; l < ctx->nlat; ++l) kappa_of_lat[l] = L[l].kappa;
   }
   return GH_OK;
