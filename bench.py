@@ -528,6 +528,7 @@ def run_extra(a, dist):
                 tiers.setdefault(nmd_for(k), []).append((b, k))
         for frozen, prec in ((False, "fp64"), (False, "fp32"), (True, "fp64")):
             K, total_s, acc = 20, 0.0, []
+            enss = []
             for nmd, pts in sorted(tiers.items()):
                 rep = gh.GeneralRep(2, [12])
                 ens = gh.Ensemble([[2] * 4] * len(pts), rep, seeds=[20260602 + i for i in range(len(pts))], precision=prec,
@@ -539,9 +540,31 @@ def run_extra(a, dist):
                 if frozen:                  # the scan under GH_FROZEN: |phi_x| = 1
                     ens.frozen_phi = True
                     ens.normalize_phi()
-                v, rec = gpu_rate(ens, K, W=20)
+                v, rec = gpu_rate(ens, K, W=20)          # this tier alone
                 total_s += K / v
                 acc.append(float(rec["accepted"].mean()))
+                enss.append(ens)
+            # the tiers are independent ensembles: all of them at once, one stream each
+            streams = [torch.cuda.Stream() for _ in enss]
+            for ens, st in zip(enss, streams):
+                ens.set_stream(st.cuda_stream)
+                ens.enqueue(2)
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            ends = []
+            for ens, st in zip(enss, streams):
+                st.wait_event(e0)
+                ens.enqueue(K)
+                ev = torch.cuda.Event()
+                ev.record(st)
+                ends.append(ev)
+            for ev in ends:
+                stream.wait_event(ev)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            conc_s = e0.elapsed_time(e1) / 1e3
+            for ens in enss:
                 ens.close()
             cpu = None
             if prec == "fp64" and ref is not None:
@@ -564,8 +587,10 @@ def run_extra(a, dist):
             out.append({"workload": "2I phase scan: SU(2) {12} 2^4, multi-invariant potential, beta 1.0..3.0 x kappa "
                                     "0.0..1.0 (99 points), Omelyan nmd 16..68 by kappa, one ensemble per nmd tier"
                                     + (", frozen |phi| = 1 (GH_FROZEN)" if frozen else ""),
-                        "precision": prec, "value": round(99 * K / total_s, 1),
-                        "unit": "point trajectories/s", "acceptance_by_tier": [round(x, 3) for x in acc],
+                        "precision": prec, "value": round(99 * K / conc_s, 1),
+                        "unit": "point trajectories/s (the five tier ensembles on five streams at once)",
+                        "one_tier_at_a_time": round(99 * K / total_s, 1),
+                        "acceptance_by_tier": [round(x, 3) for x in acc],
                         "cpu_baseline": cpu})
     if wl in ("big", "all"):
         for prec in ("fp64", "fp32"):
