@@ -527,3 +527,37 @@ def test_trajectory_host_matches_device_chain(precision):
         assert np.array_equal(phi.astype(np.complex64), hB.phi.astype(np.complex64))
     hA.close()
     hB.close()
+
+
+def test_contexts_on_concurrent_streams_match_sequential():
+    """Independent contexts share no device state: two ensembles enqueued at once on two
+    CUDA streams give bit for bit the records and fields of running them one after the
+    other on their own streams."""
+    import torch
+    import gauge_higgs_b200 as gh
+
+    def make(kappa0):
+        ens = gh.Ensemble([[4, 4, 4, 4], [4, 4, 2, 6]], gh.FundamentalRep(2), seeds=[3, 4], precision="fp32",
+                          beta=2.3, kappa=[kappa0, kappa0 + 0.02], lam=0.5, nmd=8)
+        ens.hot(0.6)
+        ens.phi_gaussian(12345, 0.4)
+        return ens
+
+    ref = []
+    for k0 in (0.2, 0.25):
+        e = make(k0)
+        ref.append(e.run(6))
+        e.close()
+    a, b = make(0.2), make(0.25)
+    sa, sb = torch.cuda.Stream(), torch.cuda.Stream()
+    a.set_stream(sa.cuda_stream)
+    b.set_stream(sb.cuda_stream)
+    a.enqueue(6)
+    b.enqueue(6)
+    torch.cuda.synchronize()
+    for e, rec in zip((a, b), ref):
+        got = e.records(6)
+        for k in ("dH", "accepted", "plaquette", "L_phi", "L_link"):
+            assert np.array_equal(got[k], rec[k]), k
+    a.close()
+    b.close()
