@@ -526,7 +526,7 @@ __device__ void gen_apply(const GenTables& t, const Mat<N, C>& M, bool dag, cons
     const int blk = t.powN[k];
     const unsigned mag = t.pmag[k];
     // fibre f = hi * blk + lo starts at hi * blk * N + lo.  Odd N in FP64 with more than
-    // two fibres per lane walks them as f = lo * N^(n-1-k) + hi instead (consecutive
+    // 64 fibres per slot (over two per lane) walks them as f = lo * N^(n-1-k) + hi instead (consecutive
     // lanes step hi): the same fibres, each computed alike, so the results do not change;
     // SU(3) 27-plet FP64 trajectories +8%, while the sextet, the octet and FP32 ran 1-4%
     // slower with it, so they keep the plain order

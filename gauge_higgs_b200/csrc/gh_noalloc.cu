@@ -18,8 +18,14 @@
 //    streams, or different host threads) race on it;
 //  - the first call on a device looks up the array's device address
 //    (cudaGetSymbolAddress, with that device current) and caches it; make that
-//    first call before any stream capture.
+//    first call before any stream capture.  The cached address belongs to the
+//    device's primary context: it does not survive cudaDeviceReset (or any other
+//    teardown of that context) — a process that resets a device must not call
+//    this entry point on it afterwards;
+//  - U_dev must be 16-byte aligned (it is read as complex FP64 pairs) and out_dev
+//    8-byte aligned; other pointers are refused with GH_ERR_ARG before any launch.
 #include <cuda_runtime.h>
+#include <stdint.h>
 #include <mutex>
 #include <string>
 #include "gh_math.cuh"
@@ -110,16 +116,23 @@ const char* gh_noalloc_last_error(void) { return g_na_err.c_str(); }
 int gh_plaquette_noalloc(int D, int N, const int* L, const double* U_dev, double* out_dev, void* stream) {
   if (D < 2 || D > 4 || N < 2 || N > 3) return na_fail(GH_ERR_UNSUPPORTED, "D must be 2..4 and N 2..3");
   if (!L || !U_dev || !out_dev) return na_fail(GH_ERR_ARG, "null argument");
+  // the links are read as 16-byte complex pairs and the outputs written as doubles: a
+  // misaligned pointer would raise a sticky misaligned-address error that ends the
+  // caller's CUDA context, so it is refused here instead
+  if ((reinterpret_cast<uintptr_t>(U_dev) & 15u) != 0)
+    return na_fail(GH_ERR_ARG, "U_dev must be 16-byte aligned (complex FP64 pairs)");
+  if ((reinterpret_cast<uintptr_t>(out_dev) & 7u) != 0) return na_fail(GH_ERR_ARG, "out_dev must be 8-byte aligned");
   Geo g{};
   long long V = 1;
   for (int mu = 0; mu < 4; ++mu) { g.L[mu] = 1; g.stride[mu] = 0; }
   for (int mu = 0; mu < D; ++mu) {
     if (L[mu] < 1) return na_fail(GH_ERR_ARG, "lattice extents must be >= 1");
+    // compared before multiplying, so that no product of extents can overflow
+    if (V > GH_NOALLOC_MAX_SITES / L[mu])
+      return na_fail(GH_ERR_ARG, "lattice has more sites than gh_plaquette_noalloc handles: at most " +
+                                     std::to_string(GH_NOALLOC_MAX_SITES) + " (its fixed scratch array)");
     g.L[mu] = L[mu]; g.stride[mu] = (int)V; V *= L[mu];
   }
-  if (V > GH_NOALLOC_MAX_SITES)
-    return na_fail(GH_ERR_ARG, "lattice has " + std::to_string(V) + " sites; gh_plaquette_noalloc handles at most " +
-                                   std::to_string(GH_NOALLOC_MAX_SITES) + " (its fixed scratch array)");
   g.V = (int)V;
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);

@@ -259,6 +259,10 @@ const char* gh_mlp_last_error(void);
  * rejected with GH_ERR_ARG.  All calls on a device share that array: calls that
  * overlap on the GPU race.  The first call on a device looks up the array's
  * device address with that device current: make it before any stream capture.
+ * That address is cached for the life of the process and belongs to the device's
+ * primary context: after cudaDeviceReset on a device, do not call this entry point
+ * on that device again.  U_dev must be 16-byte aligned and out_dev 8-byte aligned
+ * (refused with GH_ERR_ARG otherwise, before any launch).
  * Errors: message in gh_noalloc_last_error(). */
 #define GH_NOALLOC_MAX_SITES (8192 * 128)
 int gh_plaquette_noalloc(int D, int N, const int* L, const double* U_dev, double* out_dev, void* stream);

@@ -26,6 +26,7 @@
 #include <sstream>
 #include <stdexcept>
 #include <string>
+#include <numeric>
 #include <vector>
 #include "gauge_higgs_b200.h"
 
@@ -424,45 +425,48 @@ class ReplicaTempering {
   std::vector<std::uint64_t> rung_traj_, rung_acc_;
 };
 
-// ---- time-series statistics (src/measure/observables.hpp:104-145) ----
+// ---- time-series statistics (the quantities of src/measure/observables.hpp:104-145) ----
+// Written from the definitions: population moments about the sample mean, chi = V Var,
+// the Binder cumulant U4 = 1 - m4 / (3 m2^2), and the jackknife error of the mean over
+// contiguous bins.  The bin rule is the reference's (it fixes the printed error bars):
+// nbins bins of floor(n / nbins) samples from the start of the series (a remainder at
+// the end is left out), nbins lowered to max(2, n / 2) for a series shorter than
+// 2 nbins, and no error for n < 2.
 struct Stats {
   std::vector<double> x;
   void add(double v) { x.push_back(v); }
   int n() const { return (int)x.size(); }
-  double mean() const { double s = 0.0; for (double v : x) s += v; return x.empty() ? 0.0 : s / x.size(); }
-  double var() const {
-    const double m = mean();
-    double s2 = 0.0;
-    for (double v : x) s2 += v * v;
-    return x.empty() ? 0.0 : s2 / x.size() - m * m;
-  }
-  double susceptibility(double volume) const { return volume * var(); }
-  double binder() const {
+  double mean() const { return x.empty() ? 0.0 : std::accumulate(x.begin(), x.end(), 0.0) / (double)x.size(); }
+  // k-th moment about the mean, 1/n normalisation
+  double central_moment(int k) const {
     if (x.empty()) return 0.0;
     const double m = mean();
-    double m2 = 0.0, m4 = 0.0;
-    for (double v : x) { const double d = v - m; m2 += d * d; m4 += d * d * d * d; }
-    m2 /= x.size(); m4 /= x.size();
-    return m2 > 0.0 ? 1.0 - m4 / (3.0 * m2 * m2) : 0.0;
+    double acc = 0.0;
+    for (double v : x) acc += std::pow(v - m, k);
+    return acc / (double)x.size();
+  }
+  double var() const { return central_moment(2); }
+  double susceptibility(double volume) const { return volume * var(); }
+  double binder() const {
+    const double m2 = central_moment(2);
+    return m2 > 0.0 ? 1.0 - central_moment(4) / (3.0 * m2 * m2) : 0.0;
   }
   double binned_error(int nbins = 16) const {
-    const int N = n();
-    if (N < 2 * nbins) nbins = std::max(2, N / 2);
-    if (N < 2) return 0.0;
-    const int bs = N / nbins;
-    std::vector<double> bm;
-    for (int b = 0; b < nbins; ++b) {
-      double s = 0.0;
-      for (int i = b * bs; i < (b + 1) * bs; ++i) s += x[i];
-      bm.push_back(s / bs);
-    }
-    double mb = 0.0;
-    for (double v : bm) mb += v;
-    mb /= bm.size();
-    double v = 0.0;
-    for (double b : bm) v += (b - mb) * (b - mb);
-    v /= (bm.size() - 1);
-    return std::sqrt(v / bm.size());
+    const int total = n();
+    if (total < 2) return 0.0;
+    const int nb = total < 2 * nbins ? std::max(2, total / 2) : nbins;
+    const int width = total / nb;
+    // leave-one-bin-out means theta_b; error^2 = (nb - 1)/nb * sum_b (theta_b - <theta>)^2
+    std::vector<double> bin_sum(nb, 0.0);
+    for (int b = 0; b < nb; ++b)
+      bin_sum[b] = std::accumulate(x.begin() + (size_t)b * width, x.begin() + (size_t)(b + 1) * width, 0.0);
+    const double all = std::accumulate(bin_sum.begin(), bin_sum.end(), 0.0);
+    std::vector<double> theta(nb);
+    for (int b = 0; b < nb; ++b) theta[b] = (all - bin_sum[b]) / ((double)(nb - 1) * width);
+    const double tbar = std::accumulate(theta.begin(), theta.end(), 0.0) / nb;
+    double ss = 0.0;
+    for (double t : theta) ss += (t - tbar) * (t - tbar);
+    return std::sqrt((double)(nb - 1) / nb * ss);
   }
 };
 
