@@ -1,7 +1,8 @@
 #!/usr/bin/env python
 """Headline benchmark: SU(3) + fundamental-Higgs HMC on a 16^4 lattice,
-trajectories per second, FP32-MD (FP64 Hamiltonian) against the FP64 path on
-the same GPU, with the dominant kernel's roofline.
+trajectories per second, FP32-MD (FP32 fields and forces; FP64 exp(i eps P),
+SU(N) projection and Hamiltonian) against the FP64 path on the same GPU, each
+also end to end through the public API, with the dominant kernel's roofline.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
@@ -189,64 +190,73 @@ def run_ours(a, dist):
         ms = dist.max(e0.elapsed_time(e1))
         return ms, clocks
 
-    def kernel_ms(h, which, n=40):
-        eps = 0.0   # zero step: the kernel does all its work but leaves the state unchanged (kick)
-        fn = h.kick if which == "kick" else h.drift
-        for _ in range(3):
-            fn(eps)
+    def kernel_ms(h, n=8):
+        """Average device time of one kick and one drift launch as they run inside a
+        trajectory: an Omelyan-like sequence of kicks and drifts on the evolving fields
+        (L2 as the MD leaves it), CUDA events around every launch on the launching stream."""
+        eps = WL["tau"] / WL["nmd"]
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(4 * n)]
+        h.kick(0.5 * eps)
+        h.drift(0.5 * eps)
         torch.cuda.synchronize()
-        e0 = torch.cuda.Event(enable_timing=True)
-        e1 = torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        for _ in range(n):
-            fn(eps)
-        e1.record(stream)
+        for i in range(n):
+            for j, fn in enumerate((h.kick, h.drift, h.kick, h.drift)):
+                e0, e1 = ev[4 * i + j]
+                e0.record(stream)
+                fn(eps if j % 2 == 0 else 0.5 * eps)
+                e1.record(stream)
         torch.cuda.synchronize()
-        return e0.elapsed_time(e1) / n
+        t = [e0.elapsed_time(e1) for e0, e1 in ev]
+        return float(np.mean(t[0::2])), float(np.mean(t[1::2]))
 
+    def e2e_rate(h, K):
+        """End to end through the public API: gh_trajectory_host with pinned host U and phi
+        copied in every trajectory, the record and (after an accepted trajectory) U and phi
+        copied back."""
+        U_host = torch.empty(V * 4 * 9 * 2, dtype=torch.float64, pin_memory=True).numpy()
+        phi_host = torch.empty(V * 3 * 2, dtype=torch.float64, pin_memory=True).numpy()
+        Uc = U_host.view(np.complex128).reshape(V, 4, 3, 3)
+        pc = phi_host.view(np.complex128).reshape(V, 3)
+        Uc[:] = h.U
+        pc[:] = h.phi
+        Ke = max(1, min(K, 50))
+        for _ in range(2):
+            h.trajectory_host(Uc, pc)
+        torch.cuda.synchronize()
+        dist.barrier()
+        n_acc = 0
+        t0 = time.perf_counter()
+        for _ in range(Ke):
+            n_acc += int(h.trajectory_host(Uc, pc).accepted)
+        torch.cuda.synchronize()
+        e2e_s = dist.max(time.perf_counter() - t0)
+        # U and phi come back only after an accepted trajectory (a rejected one leaves the
+        # host fields as they were passed in); the record (56 B) and the lattice's descriptor
+        # with its trajectory counter (160 B) always
+        rec_bytes = 56 + 160
+        return {"value": round(dist.world * Ke / e2e_s, 3), "unit": "trajectories/s",
+                "h2d_bytes_per_step": int(U_host.nbytes + phi_host.nbytes),
+                "d2h_bytes_per_step": int(round(n_acc / Ke * (U_host.nbytes + phi_host.nbytes))) + rec_bytes,
+                "steps": Ke, "accepted": n_acc,
+                "api": "gh_trajectory_host (pinned host U, phi in; record, and U, phi when accepted, out)"}
+
+    V = int(np.prod(WL["L"]))
     K, W = a.steps, a.warmup
     res = {}
-    for prec in ("fp32", "fp64"):
+    for prec in ("fp32", "fp64", "fp32-all"):
         h = make(prec)
         sampler = ClockSampler(dist.local) if prec == "fp32" else None
         ms, clocks = timed(h, K, W, sampler)
         recs = h.records(min(K, 1024))
         res[prec] = dict(ms=ms, clocks=clocks, acc=float(np.mean(recs["accepted"])), tile=h.get_tile(),
-                         plaq=float(np.mean(recs["plaquette"])), dH=float(np.mean(recs["dH"])),
-                         kick_ms=kernel_ms(h, "kick"), drift_ms=kernel_ms(h, "drift"), h=h)
+                         plaq=float(np.mean(recs["plaquette"])), dH=float(np.mean(recs["dH"])), h=h)
+        if prec != "fp32-all":
+            res[prec]["e2e"] = e2e_rate(h, K)
+        res[prec]["kick_ms"], res[prec]["drift_ms"] = kernel_ms(h)
 
-    V = int(np.prod(WL["L"]))
-    traj_fp32 = dist.world * K / (res["fp32"]["ms"] / 1e3)
-    traj_fp64 = dist.world * K / (res["fp64"]["ms"] / 1e3)
-
-    # ---- end to end through the public API with host-resident fields ----
-    h = res["fp32"]["h"]
-    U_host = torch.empty(V * 4 * 9 * 2, dtype=torch.float64, pin_memory=True).numpy()
-    phi_host = torch.empty(V * 3 * 2, dtype=torch.float64, pin_memory=True).numpy()
-    Uc = U_host.view(np.complex128).reshape(V, 4, 3, 3)
-    pc = phi_host.view(np.complex128).reshape(V, 3)
-    Uc[:] = h.U
-    pc[:] = h.phi
-    Ke = max(1, min(K, 50))
-    for _ in range(2):
-        h.trajectory_host(Uc, pc)
-    torch.cuda.synchronize()
-    dist.barrier()
-    n_acc = 0
-    t0 = time.perf_counter()
-    for _ in range(Ke):
-        n_acc += int(h.trajectory_host(Uc, pc).accepted)
-    torch.cuda.synchronize()
-    e2e_s = dist.max(time.perf_counter() - t0)
-    # U and phi come back only after an accepted trajectory (a rejected one leaves the
-    # host fields as they were passed in); the record (56 B) and the lattice's descriptor with
-    # its trajectory counter (160 B) always
-    rec_bytes = 56 + 160
-    e2e = {"value": dist.world * Ke / e2e_s, "unit": "trajectories/s",
-           "h2d_bytes_per_step": int(U_host.nbytes + phi_host.nbytes),
-           "d2h_bytes_per_step": int(round(n_acc / Ke * (U_host.nbytes + phi_host.nbytes))) + rec_bytes,
-           "steps": Ke, "accepted": n_acc,
-           "api": "gh_trajectory_host (pinned host U, phi in; record, and U, phi when accepted, out)"}
+    rate = {p: dist.world * K / (res[p]["ms"] / 1e3) for p in res}
+    traj_fp32, traj_fp64 = rate["fp32"], rate["fp64"]
+    e2e = res["fp32"]["e2e"]
 
     # ---- roofline of the dominant kernel (FP32-MD path) ----
     hbm, peak_kind = peaks()
@@ -270,14 +280,18 @@ def run_ours(a, dist):
                "achieved": round(kick_tflops, 2), "peak": round(fp32_peak, 1), "unit": "TFLOP/s",
                "frac": round(kick_tflops / fp32_peak, 4),
                "peak_source": "nominal FP32 FMA rate at the sampled SM clock (148 SMs x 128 lanes x 2)"}
-    roofline = {"bound": "hbm", "kernel": f"k_kick<4,3,float,FUND>" if dom == "kick" else "k_drift<3,float>",
+    roofline = {"bound": "hbm", "kernel": "k_kick<4,3,float,FUND>" if dom == "kick" else "k_drift<3,float,double>",
                 "achieved": round(achieved, 1), "peak": hbm, "unit": "GB/s", "frac": round(achieved / hbm, 4),
                 "peak_source": peak_kind, "traffic": traffic,
                 "alg_bytes_per_launch": V * ALG_BYTES[dom]["fp32"], "avg_launch_ms": round(dom_ms, 5),
+                "launch_timing": "CUDA events around each kick / drift of an Omelyan sequence on the evolving fields",
                 "share_of_trajectory": round((share_kick if dom == "kick" else share_drift) / (r["ms"] / K), 3),
                 "fp64": {"kick_ms": round(res["fp64"]["kick_ms"], 5), "drift_ms": round(res["fp64"]["drift_ms"], 5),
                          "kick_GBps": round(V * ALG_BYTES["kick"]["fp64"] / (res["fp64"]["kick_ms"] / 1e3) / 1e9, 1)},
-                "fp32": {"kick_ms": round(r["kick_ms"], 5), "drift_ms": round(r["drift_ms"], 5)},
+                "fp32": {"kick_ms": round(r["kick_ms"], 5), "drift_ms": round(r["drift_ms"], 5),
+                         "drift_GBps": round(V * ALG_BYTES["drift"]["fp32"] / (r["drift_ms"] / 1e3) / 1e9, 1)},
+                "fp32_all": {"kick_ms": round(res["fp32-all"]["kick_ms"], 5),
+                             "drift_ms": round(res["fp32-all"]["drift_ms"], 5)},
                 "compute": compute}
 
     # ---- CPU baseline: the reference itself on this host's cores (rank 0, N=1) ----
@@ -288,23 +302,29 @@ def run_ours(a, dist):
     line = {
         "metric": METRIC, "value": round(traj_fp32, 3), "unit": "trajectories/s", "n_gpus": dist.world,
         "steps": K, "warmup": W, "ms_per_step": round(res["fp32"]["ms"] / K, 4), "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64",
         "data": "synthetic (reference counter-RNG hot start and Gaussian scalar field)",
         "config": {"workload": WORKLOAD, "lattice": WL["L"], "rep": "fundamental", "beta": WL["beta"],
                    "kappa": WL["kappa"], "lambda": WL["lam"], "integrator": "omelyan", "nmd": WL["nmd"],
-                   "tau": WL["tau"], "precision": "FP32 MD (fields, forces, exp(i eps P), SU(N) projection); FP64 H and Metropolis",
+                   "tau": WL["tau"],
+                   "precision": ("FP32-MD: FP32 fields, forces and kicks; each drift's exp(i eps P), product "
+                                 "with U and Gram-Schmidt SU(N) projection in FP64; FP64 H and Metropolis"),
                    "l2": "flushed between trajectories (256 MB write, inside the timed region)",
                    "kick_tile": {"fp32": res["fp32"]["tile"], "fp64": res["fp64"]["tile"]},
                    "parallelism": f"replicas x{dist.world}"},
         "fp64": {"value": round(traj_fp64, 3), "ms_per_step": round(res["fp64"]["ms"] / K, 4),
-                 "acceptance": res["fp64"]["acc"], "plaquette": res["fp64"]["plaq"]},
+                 "acceptance": res["fp64"]["acc"], "plaquette": res["fp64"]["plaq"], "e2e": res["fp64"]["e2e"],
+                 "dtype": "f64"},
+        "fp32_all": {"value": round(rate["fp32-all"], 3), "ms_per_step": round(res["fp32-all"]["ms"] / K, 4),
+                     "acceptance": res["fp32-all"]["acc"], "plaquette": res["fp32-all"]["plaq"],
+                     "precision": "non-default variant: the drift's exponential and projection in FP32 too"},
         "fp32_over_fp64": round(traj_fp32 / traj_fp64, 3),
         "acceptance": res["fp32"]["acc"], "plaquette": res["fp32"]["plaq"],
         "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
         "gpu_launches": K * launches_per_traj(WL["nmd"], "fp32"),
         "clocks": res["fp32"]["clocks"],
     }
-    for p in ("fp32", "fp64"):
+    for p in res:
         res[p]["h"].close()
     dist.close()
     if dist.rank == 0:

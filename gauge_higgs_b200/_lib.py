@@ -16,7 +16,7 @@ GH_OK = 0
 ERRORS = {-1: "GH_ERR_ARG", -2: "GH_ERR_CUDA", -3: "GH_ERR_REP", -4: "GH_ERR_STATE", -5: "GH_ERR_NONFINITE",
           -6: "GH_ERR_UNSUPPORTED"}
 REP_NONE, REP_FUND, REP_ADJ, REP_GENERAL = 0, 1, 2, 3
-PREC_FP64, PREC_FP32_MD = 0, 1
+PREC_FP64, PREC_FP32_MD, PREC_FP32_ALL = 0, 1, 2
 LEAPFROG, OMELYAN = 0, 1
 
 

@@ -133,7 +133,9 @@ void enq_kick(gh_ctx* ctx, double eps) {
   ctx->eng->kick(ctx->b, eps, M_UPDATE, F_GAUGE | F_MATTER, nullptr, true, true);
   if (ctx->b.frozen) ctx->eng->sphere(ctx->b, 0);   // drop the radial force (src/hmc/gauge_higgs_hmc.hpp:133)
 }
-void enq_drift(gh_ctx* ctx, double eps) { ctx->eng->drift(ctx->b, eps, ctx->prec == GH_PREC_FP32_MD ? 1 : 0); }
+void enq_drift(gh_ctx* ctx, double eps) {
+  ctx->eng->drift(ctx->b, eps, ctx->prec == GH_PREC_FP32_MD ? 1 : ctx->prec == GH_PREC_FP32_ALL ? 2 : 0);
+}
 
 // md_evolve: src/hmc/gauge_higgs_hmc.hpp:149-165 (identical in src/hmc/hmc.hpp:54-70)
 void enq_md(gh_ctx* ctx) {
@@ -482,7 +484,8 @@ int gh_ctx_create(int D, int N, int n_lat, const int* L, const gh_rep_desc* rep,
   if (D < 2 || D > 4) return fail(nullptr, GH_ERR_UNSUPPORTED, "D must be 2, 3 or 4");
   if (N < 2 || N > 3) return fail(nullptr, GH_ERR_UNSUPPORTED, "N must be 2 or 3");
   if (n_lat < 1 || !L || !seeds) return fail(nullptr, GH_ERR_ARG, "need n_lat >= 1, extents and seeds");
-  if (precision != GH_PREC_FP64 && precision != GH_PREC_FP32_MD) return fail(nullptr, GH_ERR_ARG, "unknown precision");
+  if (precision != GH_PREC_FP64 && precision != GH_PREC_FP32_MD && precision != GH_PREC_FP32_ALL)
+    return fail(nullptr, GH_ERR_ARG, "unknown precision");
   int dev_count = 0;
   if (cudaGetDeviceCount(&dev_count) != cudaSuccess || dev_count == 0) {
     cudaGetLastError();

@@ -53,6 +53,7 @@ struct EngineBase {
   virtual ~EngineBase() {}
   virtual void kick(const Bufs& b, double eps, int mode, int flags, double* out, bool links, bool sites) = 0;
   virtual void gen_links(const Bufs& b, double eps, int mode, double* out) = 0;
+  // reunit: 0 none (FP64 mode), 1 projection in FP64 arithmetic, 2 the all-FP32 update
   virtual void drift(const Bufs& b, double eps, int reunit) = 0;
   virtual void reunit(const Bufs& b) = 0;
   virtual void sphere(const Bufs& b, int what) = 0;
@@ -104,8 +105,11 @@ struct Engine : EngineBase {
   void drift(const Bufs& b, double eps, int reunit) override {
     DriftArgs a;
     a.work = b.w_all; a.lats = b.lats; a.U = b.U; a.P = b.P; a.phi = b.phi; a.pi = b.pi;
-    a.eps = eps; a.reunit = reunit; a.d = b.d; a.frozen = b.frozen;
-    launch(k_drift<N, R>, b.nw_links + (b.scalar ? b.nw_sites : 0), KBLOCK, 0, b.st, a);
+    a.eps = eps; a.reunit = reunit != 0; a.d = b.d; a.frozen = b.frozen;
+    const unsigned nb = b.nw_links + (b.scalar ? b.nw_sites : 0);
+    // reunit 2: the all-FP32 link update (GH_PREC_FP32_ALL); otherwise FP64 arithmetic
+    if (sizeof(R) != sizeof(double) && reunit == 2) launch(k_drift<N, R, float>, nb, KBLOCK, 0, b.st, a);
+    else launch(k_drift<N, R, double>, nb, KBLOCK, 0, b.st, a);
   }
   void sphere(const Bufs& b, int what) override {
     if (!b.scalar) return;

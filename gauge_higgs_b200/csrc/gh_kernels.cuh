@@ -739,10 +739,17 @@ __global__ void __launch_bounds__(GEN_WARPS * 32) k_gen_links(const GenArgs a) {
 }
 
 // ---------------------------------------------------------------------------
-// Drift: U <- exp(i eps P) U (src/hmc/gauge_higgs_hmc.hpp:136-143), with the
-// exponential and the product in the storage precision of the links (FP64 mode:
-// FP64; FP32-MD: FP32); optional projection back to SU(N) (FP32-MD mode projects
-// every step).  Site items: phi += eps pi (:145-146).
+// Drift: U <- exp(i eps P) U (src/hmc/gauge_higgs_hmc.hpp:136-143); site items:
+// phi += eps pi (:145-146).  The link update (exponential, product with U,
+// projection) runs in the arithmetic type A, whatever the storage type R:
+//   FP64 mode       R = double, A = double, no projection (the reference's
+//                   reunitarisation once per trajectory, k_reunit);
+//   FP32-MD         R = float,  A = double: FP32 links and momenta are widened,
+//                   exp(i eps P) (scaling, Cayley-Hamilton series), its product
+//                   with U and the Gram-Schmidt projection back to SU(N) are
+//                   FP64, the result is rounded to FP32 once;
+//   FP32-MD, all    R = float,  A = float: the same steps in FP32 (non-default
+//   FP32            variant, GH_PREC_FP32_ALL).
 // ---------------------------------------------------------------------------
 // Projection back to SU(N) after each FP32-MD drift: Gram-Schmidt on the first
 // N-1 rows, the last row fixed by det = 1 (SU(2): (-conj u01, conj u00); SU(3):
@@ -795,7 +802,7 @@ struct DriftArgs {
   int d;
   int frozen;          // |phi_x| = 1: geodesic (great-circle) drift of (phi, pi)
 };
-template <int N, typename R>
+template <int N, typename R, typename A>
 __global__ void __launch_bounds__(KBLOCK) k_drift(const DriftArgs a) {
   pdl_enter();
   const Work w = a.work[blockIdx.x];
@@ -806,17 +813,17 @@ __global__ void __launch_bounds__(KBLOCK) k_drift(const DriftArgs a) {
     const int mu = w.mu;
     constexpr int ng = N * N - 1;
     const R* P = (const R*)a.P;
-    R v[ng];
+    A v[ng];
     const long long pb = p_index(L, ng, mu, 0, s);
 #pragma unroll
-    for (int g = 0; g < ng; ++g) v[g] = P[pb + g * ULANE];
-    Mat<N, R> H = alg_to_mat<N, R>(v);
+    for (int g = 0; g < ng; ++g) v[g] = (A)P[pb + g * ULANE];
+    Mat<N, A> H = alg_to_mat<N, A>(v);
 #pragma unroll
-    for (int i = 0; i < N * N; ++i) H.e[i] = scale(H.e[i], (R)a.eps);
-    const Mat<N, R> E = expi<N>(H);
-    Mat<N, R> Un = mm(E, ld_link_rw<N, R>((const R*)a.U, L, mu, s));
-    if (a.reunit) project_su<N, R>(Un);
-    st_link<N, R>((R*)a.U, L, mu, s, Un);
+    for (int i = 0; i < N * N; ++i) H.e[i] = scale(H.e[i], (A)a.eps);
+    const Mat<N, A> E = expi<N>(H);
+    Mat<N, A> Un = mm(E, ld_link_rw<N, A>((const R*)a.U, L, mu, s));
+    if (a.reunit) project_su<N, A>(Un);
+    st_link<N, A>((R*)a.U, L, mu, s, Un);
   } else if (a.frozen) {
     // Frozen length (src/hmc/gauge_higgs_hmc.hpp:84-102): the exact constrained free
     // flow on the unit sphere, r = |pi|:

@@ -314,6 +314,28 @@ GH_HD double inv_int(int n) {
     case 18: return 1.0 / 18.0; case 19: return 1.0 / 19.0; case 20: return 0.05; default: return 1.0 / n;
   }
 }
+// Q^2 of a Hermitian 3x3 Q: the diagonal is the squared row norms, the upper
+// triangle three complex dot products, the lower triangle their conjugates (54
+// multiply-adds instead of the general product's 108).
+template <typename T> GH_HD Mat<3, T> herm_sq3(const Mat<3, T>& Q) {
+  Mat<3, T> R;
+#pragma unroll
+  for (int i = 0; i < 3; ++i) {
+    T d = T(0);
+#pragma unroll
+    for (int k = 0; k < 3; ++k) d = fmad(Q.e[i * 3 + k].re, Q.e[i * 3 + k].re, fmad(Q.e[i * 3 + k].im, Q.e[i * 3 + k].im, d));
+    R.e[i * 4] = mk<T>(d, T(0));
+#pragma unroll
+    for (int j = i + 1; j < 3; ++j) {
+      cx<T> z = zero<T>();
+#pragma unroll
+      for (int k = 0; k < 3; ++k) z = cfma(z, Q.e[i * 3 + k], Q.e[k * 3 + j]);
+      R.e[i * 3 + j] = z;
+      R.e[j * 3 + i] = conj(z);
+    }
+  }
+  return R;
+}
 template <typename T> GH_HD Mat<3, T> expi3(const Mat<3, T>& H) {
   T nrm2 = fnorm2(H);               // scale until ||H||_F / 2^s <= 1/2, compared squared
   int s = 0;
@@ -322,7 +344,7 @@ template <typename T> GH_HD Mat<3, T> expi3(const Mat<3, T>& H) {
   Mat<3, T> Q;
 #pragma unroll
   for (int i = 0; i < 9; ++i) Q.e[i] = scale(H.e[i], sc);
-  const Mat<3, T> Q2 = mm(Q, Q);
+  const Mat<3, T> Q2 = herm_sq3(Q);   // H (and Q) Hermitian: built from real algebra coefficients
   const T c1 = T(0.5) * (Q2.e[0].re + Q2.e[4].re + Q2.e[8].re);
   const T c0 = det<3, T>(Q).re;
   T a = 1, b = 0, g = 0, coef = 1;

@@ -23,7 +23,9 @@ int main(int argc, char** argv) {
   const double tau = argf(6, 1.0);
   const std::uint64_t seed = (std::uint64_t)argi(7, 1);
   const char* pe = std::getenv("GH_PRECISION");
-  const ghb::Precision prec = (pe && std::strcmp(pe, "fp32") == 0) ? ghb::Precision::FP32_MD : ghb::Precision::FP64;
+  const ghb::Precision prec = (pe && std::strcmp(pe, "fp32") == 0)       ? ghb::Precision::FP32_MD
+                               : (pe && std::strcmp(pe, "fp32-all") == 0) ? ghb::Precision::FP32_ALL
+                                                                          : ghb::Precision::FP64;
   std::array<int, kDim> L{};
   for (int mu = 0; mu < kDim; ++mu) L[mu] = Lext;
   try {

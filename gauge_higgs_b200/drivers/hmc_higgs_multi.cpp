@@ -59,7 +59,9 @@ int main(int argc, char** argv) {
     }
     const bool frozen = std::getenv("GH_FROZEN") != nullptr;   // |phi_x| = 1 frozen-length scalar
     const char* pe = std::getenv("GH_PRECISION");
-    const ghb::Precision prec = (pe && std::strcmp(pe, "fp32") == 0) ? ghb::Precision::FP32_MD : ghb::Precision::FP64;
+    const ghb::Precision prec = (pe && std::strcmp(pe, "fp32") == 0)       ? ghb::Precision::FP32_MD
+                               : (pe && std::strcmp(pe, "fp32-all") == 0) ? ghb::Precision::FP32_ALL
+                                                                          : ghb::Precision::FP64;
     ghb::MultiInvariantPotential<kN> pot(ch, f, mu2);
 
     std::array<int, kDim> L{};

@@ -21,8 +21,11 @@ from ._lib import LIB, check, GaugeHiggsError, RepDesc, Obs, TrajRecord, TRAJ_DT
 
 LEAPFROG, OMELYAN = _lib.LEAPFROG, _lib.OMELYAN
 _INTEG = {"leapfrog": LEAPFROG, "omelyan": OMELYAN, LEAPFROG: LEAPFROG, OMELYAN: OMELYAN}
+# "fp32" / "fp32-md": FP32 fields and forces, the drift's exp(i eps P), product and
+# SU(N) projection in FP64; "fp32-all": those in FP32 as well (non-default variant)
 _PREC = {"fp64": _lib.PREC_FP64, "fp32": _lib.PREC_FP32_MD, "fp32-md": _lib.PREC_FP32_MD,
-         _lib.PREC_FP64: _lib.PREC_FP64, _lib.PREC_FP32_MD: _lib.PREC_FP32_MD}
+         "fp32-all": _lib.PREC_FP32_ALL, _lib.PREC_FP64: _lib.PREC_FP64, _lib.PREC_FP32_MD: _lib.PREC_FP32_MD,
+         _lib.PREC_FP32_ALL: _lib.PREC_FP32_ALL}
 
 
 def _dptr(a):

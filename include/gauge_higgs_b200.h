@@ -44,7 +44,13 @@ extern "C" {
 #define GH_ERR_UNSUPPORTED -6
 
 enum { GH_REP_NONE = 0, GH_REP_FUND = 1, GH_REP_ADJ = 2, GH_REP_GENERAL = 3 };
-enum { GH_PREC_FP64 = 0, GH_PREC_FP32_MD = 1 };
+/* Precision modes.  FP64: everything FP64 (the reference's arithmetic).  FP32_MD:
+ * links, momenta, scalar fields and forces stored and computed in FP32; in every
+ * drift exp(i eps P), its product with U and the Gram-Schmidt projection back to
+ * SU(N) in FP64 (rounded to FP32 once); Hamiltonian sums and Metropolis in FP64.
+ * FP32_ALL: as FP32_MD, with the drift's exponential, product and projection in
+ * FP32 as well (a faster, non-default variant). */
+enum { GH_PREC_FP64 = 0, GH_PREC_FP32_MD = 1, GH_PREC_FP32_ALL = 2 };
 enum { GH_LEAPFROG = 0, GH_OMELYAN = 1 };
 /* How D(U) of the scalar's representation is applied on the device (gh_rep_path). */
 enum { GH_PATH_REGISTER = 0, GH_PATH_TENSOR = 1, GH_PATH_CLOSED_FORM = 2 };

@@ -37,7 +37,7 @@ inline void check(int rc, const gh_ctx* ctx) {
 }
 
 enum class Integrator { Leapfrog, Omelyan2MN };
-enum class Precision { FP64 = GH_PREC_FP64, FP32_MD = GH_PREC_FP32_MD };
+enum class Precision { FP64 = GH_PREC_FP64, FP32_MD = GH_PREC_FP32_MD, FP32_ALL = GH_PREC_FP32_ALL };
 
 // ---- representations ----
 struct Representation {

@@ -1,24 +1,26 @@
 """The C++ drivers (include/gauge_higgs_b200.hpp + gauge_higgs_b200/drivers) as a
-drop-in for the reference's own binaries, checked statistically against numbers
-the reference printed for the same command line.
+drop-in for the reference's own binaries, checked statistically against the
+reference run live on the same command line.
 
-Reference run (hmc_higgs fund 6 2.3 0.20 0.5 50 100 20 1.0 1, the reference build
-at OMP=8, recorded for this project): plaquette 0.602628 +/- 0.000886,
-L_phi 1.358482 +/- 0.001532, L_link 0.196085 +/- 0.001202, acceptance 0.98,
-<exp(-dH)> 0.99939.  A trajectory diverges from the reference's at the ULP level
-(the reference's libm is not correctly rounded), so agreement is statistical.
+`hmc_higgs fund 6 2.3 0.20 0.5 50 1000 20 1.0 1` (the CLI's Omelyan integrator,
+src/hmc_higgs.cpp:51-54) on the GPU through the C++ driver and on the reference
+(oracle/_ref, the unmodified reference headers, all host threads) with the same
+arguments.  A trajectory diverges from the reference's at the ULP level (the
+reference's libm is not correctly rounded), so agreement is statistical: each
+observable's means differ by less than 3.5 combined jackknife errors.
 """
 import os
 import re
 import subprocess
 
+import numpy as np
 import pytest
 
 from conftest import ROOT
 
 pytestmark = pytest.mark.gpu
 BIN = os.path.join(ROOT, "gauge_higgs_b200", "bin")
-REF = {"plaquette": (0.602628, 0.000886), "L_phi": (1.358482, 0.001532), "L_link": (0.196085, 0.001202)}
+NMEAS = 1000
 
 
 def parse(out):
@@ -30,18 +32,40 @@ def parse(out):
     return vals
 
 
+@pytest.fixture(scope="module")
+def ref_c1_omelyan():
+    from oracle.oracle import Reference, have_reference, OMELYAN
+    from gauge_higgs_b200.stats import Stats
+    if not have_reference():
+        pytest.fail("oracle/_ref/libghref.so (the reference harness) is not built")
+    r = Reference()
+    r.set_threads(os.cpu_count() or 1)
+    series, acc = r.run(4, 2, [6] * 4, "fund", 2.3, 0.20, 0.5, 50, NMEAS, 20, 1.0, 1, OMELYAN)
+    out = {}
+    for k, col in (("plaquette", 0), ("L_phi", 1), ("L_link", 2)):
+        st = Stats(series[:, col])
+        out[k] = (st.mean(), st.binned_error())
+    out["acceptance"] = acc
+    return out
+
+
 @pytest.mark.parametrize("precision", ["fp64", "fp32"])
-def test_hmc_higgs_c1_matches_reference_statistics(precision):
+def test_hmc_higgs_c1_matches_reference_statistics(precision, ref_c1_omelyan):
     env = dict(os.environ, GH_PRECISION=precision)
-    r = subprocess.run([os.path.join(BIN, "hmc_higgs"), "fund", "6", "2.3", "0.20", "0.5", "50", "100", "20", "1.0", "1"],
-                       capture_output=True, text=True, env=env, timeout=300)
+    r = subprocess.run([os.path.join(BIN, "hmc_higgs"), "fund", "6", "2.3", "0.20", "0.5", "50", str(NMEAS), "20",
+                        "1.0", "1"], capture_output=True, text=True, env=env, timeout=300)
     assert r.returncode == 0, r.stderr
     v = parse(r.stdout)
-    for k, (mean, err) in REF.items():
+    z = {}
+    for k in ("plaquette", "L_phi", "L_link"):
+        mean, err = ref_c1_omelyan[k]
         ours, oerr = v[k]
-        assert abs(ours - mean) < 5 * (err ** 2 + oerr ** 2) ** 0.5, (k, ours, oerr, mean, err)
-    assert v["acceptance"][0] > 0.9
-    assert abs(v["<exp(-dH)>"][0] - 1.0) < 0.1
+        z[k] = (ours - mean) / np.hypot(err, oerr)
+    print(f"\n{precision}: deviations from the reference in combined sigma: "
+          + ", ".join(f"{k} {x:+.2f}" for k, x in z.items()))
+    assert all(abs(x) < 3.5 for x in z.values()), z
+    assert abs(v["acceptance"][0] - ref_c1_omelyan["acceptance"]) < 0.03
+    assert abs(v["<exp(-dH)>"][0] - 1.0) < 0.05
     assert v["max||UdU-I||"][0] < 1e-6
 
 

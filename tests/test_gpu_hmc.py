@@ -97,7 +97,7 @@ def test_scalar_force_finite_difference(N, kind):
 # ---------------------------------------------------------------------------
 # reversibility (test_gauge.cpp:65-85, test_scalar.cpp:122-141)
 # ---------------------------------------------------------------------------
-@pytest.mark.parametrize("precision,tol", [("fp64", 1e-9), ("fp32", 2e-4)])
+@pytest.mark.parametrize("precision,tol", [("fp64", 1e-9), ("fp32", 2e-4), ("fp32-all", 2e-4)])
 @pytest.mark.parametrize("N,kind", [(2, "none"), (3, "none"), (2, "fund"), (2, "adj"), (3, "fund"), (3, "gen2")])
 def test_reversibility(N, kind, precision, tol):
     h = make(kind, 3, N, precision=precision, seed=999, beta=2.3, kappa=0.3, lam=0.5, nmd=12)
@@ -145,7 +145,7 @@ def test_fp32_refresh_equals_rounded_fp64():
 # ---------------------------------------------------------------------------
 # dH second-order scaling (test_gauge.cpp:88-107)
 # ---------------------------------------------------------------------------
-@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+@pytest.mark.parametrize("precision", ["fp64", "fp32", "fp32-all"])
 def test_dH_scaling(precision):
     def run(nmd):
         h = make("none", 3, 2, precision=precision, seed=31415, beta=2.3, nmd=nmd)
@@ -213,13 +213,55 @@ def test_fp32_force_error():
         h.close()
 
 
-def test_fp32_fp64_trajectory_agreement():
+@pytest.mark.parametrize("N", [2, 3])
+def test_fp32_md_drift_is_fp64_arithmetic(N):
+    """FP32-MD drift: exp(i eps P), its product with U and the SU(N) projection run in
+    FP64 on the FP32 fields, so one drift equals the FP64 drift of the same (rounded)
+    inputs followed by one projection to SU(N), up to the final rounding to FP32.  The
+    all-FP32 variant is only FP32-accurate."""
+    import gauge_higgs_b200 as gh
+    L = [6, 4, 4, 6]
+    rep = gh.FundamentalRep(N)
+    hs = {p: gh.GaugeHiggsHMC(L, rep, seed=11, precision=p, beta=5.7, kappa=0.1, lam=0.5)
+          for p in ("fp64", "fp32", "fp32-all")}
+    hs["fp64"].hot(0.8)
+    hs["fp64"].phi_gaussian(12345, 0.3)
+    hs["fp64"].refresh_momenta()
+    U = hs["fp64"].U.astype(np.complex64).astype(np.complex128)
+    P = hs["fp64"].P.astype(np.float32).astype(np.float64)
+    for h in hs.values():
+        h.U = U
+        h.P = P
+        h.phi = hs["fp64"].phi
+        h.drift(0.0625)
+    ref = hs["fp64"].U
+    # the FP64 reference projected to SU(N) in numpy (Gram-Schmidt, det 1)
+    M = ref.reshape(-1, N, N).copy()
+    for k in range(N - 1):
+        for j in range(k):
+            M[:, k] -= np.einsum("v,vi->vi", np.einsum("vi,vi->v", M[:, j].conj(), M[:, k]), M[:, j])
+        M[:, k] /= np.linalg.norm(M[:, k], axis=1)[:, None]
+    if N == 3:
+        M[:, 2] = np.cross(M[:, 0], M[:, 1]).conj()
+    else:
+        M[:, 1] = np.stack([-M[:, 0, 1].conj(), M[:, 0, 0].conj()], axis=1)
+    ref = M.reshape(ref.shape)
+    err_md = np.abs(hs["fp32"].U - ref).max()
+    err_all = np.abs(hs["fp32-all"].U - ref).max()
+    assert err_md < 1.5e-7, err_md              # one FP32 rounding of O(1) entries
+    assert err_all < 3e-6, err_all
+    for h in hs.values():
+        h.close()
+
+
+@pytest.mark.parametrize("p32", ["fp32", "fp32-all"])
+def test_fp32_fp64_trajectory_agreement(p32):
     """Same start, same momenta (bit-identical RNG in both modes): dH and the final
     fields of one trajectory agree to FP32 accuracy."""
     import gauge_higgs_b200 as gh
     L = [8, 8, 8, 8]
     out = {}
-    for p in ("fp64", "fp32"):
+    for p in ("fp64", p32):
         h = gh.GaugeHiggsHMC(L, gh.FundamentalRep(3), seed=7, precision=p, beta=5.7, kappa=0.1, lam=0.5, nmd=16)
         h.cold()
         h.phi_gaussian(12345, 0.3)
@@ -229,8 +271,8 @@ def test_fp32_fp64_trajectory_agreement():
         acc = h.trajectory()
         out[p] = (h.last_dH, acc, h.U, h.measure()["plaquette"])
         h.close()
-    assert abs(out["fp64"][0] - out["fp32"][0]) < 0.05 + 0.02 * abs(out["fp64"][0])
-    assert abs(out["fp64"][3] - out["fp32"][3]) < 1e-4
+    assert abs(out["fp64"][0] - out[p32][0]) < 0.05 + 0.02 * abs(out["fp64"][0])
+    assert abs(out["fp64"][3] - out[p32][3]) < 1e-4
 
 
 # ---------------------------------------------------------------------------
