@@ -190,24 +190,31 @@ def run_ours(a, dist):
         ms = dist.max(e0.elapsed_time(e1))
         return ms, clocks
 
-    def kernel_ms(h, n=8):
-        """Average device time of one kick and one drift launch as they run inside a
-        trajectory: an Omelyan-like sequence of kicks and drifts on the evolving fields
-        (L2 as the MD leaves it), CUDA events around every launch on the launching stream."""
+    def kernel_ms(h, n=40):
+        """Average device time of one kick and one drift launch, back to back as in the MD
+        (programmatic dependent launch overlapping each launch's tail with the next, the
+        fields L2-resident as inside a trajectory): n kicks at eps = 0 (the state does not
+        change), then n kick + drift pairs (the drift at the MD step); drift = pair - kick.
+        CUDA events on the launching stream around each group."""
         eps = WL["tau"] / WL["nmd"]
-        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(4 * n)]
-        h.kick(0.5 * eps)
-        h.drift(0.5 * eps)
-        torch.cuda.synchronize()
-        for i in range(n):
-            for j, fn in enumerate((h.kick, h.drift, h.kick, h.drift)):
-                e0, e1 = ev[4 * i + j]
-                e0.record(stream)
-                fn(eps if j % 2 == 0 else 0.5 * eps)
-                e1.record(stream)
-        torch.cuda.synchronize()
-        t = [e0.elapsed_time(e1) for e0, e1 in ev]
-        return float(np.mean(t[0::2])), float(np.mean(t[1::2]))
+
+        def group(fns):
+            for _ in range(3):
+                for fn, e in fns:
+                    fn(e)
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            for _ in range(n):
+                for fn, e in fns:
+                    fn(e)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            return e0.elapsed_time(e1) / n
+
+        k = group([(h.kick, 0.0)])
+        pair = group([(h.kick, 0.0), (h.drift, eps)])
+        return k, max(pair - k, 0.0)
 
     def e2e_rate(h, K):
         """End to end through the public API: gh_trajectory_host with pinned host U and phi
@@ -284,7 +291,8 @@ def run_ours(a, dist):
                 "achieved": round(achieved, 1), "peak": hbm, "unit": "GB/s", "frac": round(achieved / hbm, 4),
                 "peak_source": peak_kind, "traffic": traffic,
                 "alg_bytes_per_launch": V * ALG_BYTES[dom]["fp32"], "avg_launch_ms": round(dom_ms, 5),
-                "launch_timing": "CUDA events around each kick / drift of an Omelyan sequence on the evolving fields",
+                "launch_timing": ("CUDA events around 40 back-to-back kicks (eps 0) and 40 kick + drift pairs "
+                                  "(drift = pair - kick), fields L2-resident as inside a trajectory"),
                 "share_of_trajectory": round((share_kick if dom == "kick" else share_drift) / (r["ms"] / K), 3),
                 "fp64": {"kick_ms": round(res["fp64"]["kick_ms"], 5), "drift_ms": round(res["fp64"]["drift_ms"], 5),
                          "kick_GBps": round(V * ALG_BYTES["kick"]["fp64"] / (res["fp64"]["kick_ms"] / 1e3) / 1e9, 1)},
@@ -454,20 +462,27 @@ def run_extra(a, dist):
         c3 = {"sextet": ("sextet {2}", [2], False), "octet": ("octet {2,1}:real", [2, 1], True),
               "27plet": ("27-plet {4,2}:real", [4, 2], True)}
         for spec, rows, real in (c3[k] for k in a.c3_reps.split(",")):
+            rep = gh.GeneralRep(3, rows, real=real)
             for prec in ("fp64", "fp32"):
-                rep = gh.GeneralRep(3, rows, real=real)
-                h = gh.GaugeHiggsHMC([12] * 4, rep, seed=1, precision=prec, beta=5.7, kappa=0.1, lam=0.5, nmd=20)
-                h.hot(0.8)
-                h.phi_gaussian(12345, 1.0)
-                K = 20 if rows == [4, 2] else 50
-                v, rec = gpu_rate(h, K, W=1)
-                cpu = None
-                if prec == "fp64" and rows != [4, 2]:
-                    sp = ",".join(map(str, rows)) + (":real" if real else "")
-                    cpu = cpu_rate(4, 3, [12] * 4, sp, 5.7, 0.1, 0.5, 20, OMELYAN, 1, phi_sigma=1.0)
-                out.append({"workload": f"C3 SU(3) 12^4 {spec} beta=5.7 kappa=0.1 lambda=0.5 Omelyan nmd=20",
-                            "precision": prec, "value": round(v, 3), "unit": "trajectories/s", "cpu_baseline": cpu})
-                h.close()
+                paths = [None]
+                for path in paths:
+                    h = gh.GaugeHiggsHMC([12] * 4, rep, seed=1, precision=prec, beta=5.7, kappa=0.1, lam=0.5, nmd=20)
+                    if path is None and h.rep_path() == "product" and a.c3_ab:
+                        paths.append("tensor")       # the same workload without the product path (A/B)
+                    if path is not None:
+                        h.set_rep_path(path)
+                    h.hot(0.8)
+                    h.phi_gaussian(12345, 1.0)
+                    K = 20 if (rows == [4, 2] and h.rep_path() == "tensor") else 50
+                    v, rec = gpu_rate(h, K, W=1)
+                    cpu = None
+                    if prec == "fp64" and rows != [4, 2] and path is None:
+                        sp = ",".join(map(str, rows)) + (":real" if real else "")
+                        cpu = cpu_rate(4, 3, [12] * 4, sp, 5.7, 0.1, 0.5, 20, OMELYAN, 1, phi_sigma=1.0)
+                    out.append({"workload": f"C3 SU(3) 12^4 {spec} beta=5.7 kappa=0.1 lambda=0.5 Omelyan nmd=20",
+                                "precision": prec, "path": h.rep_path(), "value": round(v, 3), "unit": "trajectories/s",
+                                "acceptance": float(rec["accepted"].mean()), "cpu_baseline": cpu})
+                    h.close()
     if wl in ("c4", "all"):
         Ls = [6, 8, 10, 12]
         ext = [[L] * 4 for L in Ls for _ in range(16)]
@@ -686,6 +701,7 @@ def main():
     ap.add_argument("--kick-tile", default="", help="fixed kick tile (e.g. 16,2,2,2) instead of the timed choice")
     ap.add_argument("--validate-traj", type=int, default=2000)
     ap.add_argument("--validate-therm", type=int, default=200)
+    ap.add_argument("--c3-ab", action="store_true", help="C3: also time product-path irreps on the tensor path")
     ap.add_argument("--workload", default="c2", choices=["c2", "c1", "c3", "c4", "big", "stage0", "scan", "validate", "all"],
                     help="c2 (default) prints the headline line; the others print additional measurements")
     a = ap.parse_args()

@@ -13,6 +13,7 @@
 #include "gh_engine.cuh"
 #include "gh_potential.h"
 #include "gh_sympow.h"
+#include "gh_adjprod.h"
 #include "../../include/gauge_higgs_b200.h"
 
 using namespace ghk;
@@ -62,6 +63,10 @@ struct gh_ctx {
   // the tensor path or when the tensor buffer does not fit in shared memory)
   ghsym::Terms sp;
   bool use_sp = false;
+  // general irreps inside the adjoint product (gh_adjprod.h): the intertwiner Q, and
+  // whether the link kernel goes that way (gh_set_rep_path switches it)
+  ghadj::Product prod;
+  bool has_prod = false;
   size_t gen_warp_bytes = 0, gen_px_off = 0;
   // multi-invariant potential: device copies of the channel superoperator (sparse rows)
   int* sa_ptr = nullptr;
@@ -440,6 +445,23 @@ int build_general(gh_ctx* ctx, const gh_rep_desc* r) {
   if (!t_v.empty()) CK(cudaMemcpyAsync(v3, t_v.data(), t_v.size() * 16, cudaMemcpyHostToDevice, ctx->st));
   t.wt_ptr = p1; t.wt_l = p2; t.wt_v = v1; t.w_ptr = p3; t.w_i = p4; t.w_v = v2; t.t_ptr = p5; t.t_j = p6; t.t_v = v3;
   t.sp_ptr = nullptr; t.sp_c = nullptr; t.sp_e = nullptr;
+  t.pq64 = nullptr; t.pq32 = nullptr; t.pK = 0;
+  if (ctx->has_prod) {
+    const std::vector<std::complex<double>>& Q = ctx->prod.Q;
+    std::vector<double2> q64(Q.size());
+    std::vector<float2> q32(Q.size());
+    for (size_t i = 0; i < Q.size(); ++i) {
+      q64[i] = make_double2(Q[i].real(), Q[i].imag());
+      q32[i] = make_float2((float)Q[i].real(), (float)Q[i].imag());
+    }
+    double2* d64;
+    float2* d32;
+    if ((rc = dalloc(ctx, &d64, q64.size())) || (rc = dalloc(ctx, &d32, q32.size()))) return rc;
+    CK(cudaMemcpyAsync(d64, q64.data(), q64.size() * sizeof(double2), cudaMemcpyHostToDevice, ctx->st));
+    CK(cudaMemcpyAsync(d32, q32.data(), q32.size() * sizeof(float2), cudaMemcpyHostToDevice, ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));     // the host vectors go out of scope
+    t.pq64 = d64; t.pq32 = d32; t.pK = ctx->prod.K;
+  }
   t.warp_bytes = (int)ctx->gen_warp_bytes;
   t.px_off = (int)ctx->gen_px_off;
   if (ctx->use_sp) {
@@ -468,7 +490,25 @@ const char* gh_last_error(const gh_ctx* ctx) { return ctx ? ctx->err.c_str() : g
 
 int gh_rep_path(const gh_ctx* ctx, int* path) {
   if (!ctx || !path) return fail(nullptr, GH_ERR_ARG, "null argument");
-  *path = ctx->rep != REP_GEN ? GH_PATH_REGISTER : (ctx->use_sp ? GH_PATH_CLOSED_FORM : GH_PATH_TENSOR);
+  *path = ctx->rep != REP_GEN ? GH_PATH_REGISTER
+          : ctx->b.gen_prod    ? GH_PATH_PRODUCT
+          : (ctx->use_sp ? GH_PATH_CLOSED_FORM : GH_PATH_TENSOR);
+  return GH_OK;
+}
+
+int gh_set_rep_path(gh_ctx* ctx, int path) {
+  if (!ctx) return fail(nullptr, GH_ERR_ARG, "null context");
+  if (ctx->rep != REP_GEN) return path == GH_PATH_REGISTER ? GH_OK : fail(ctx, GH_ERR_ARG, "not a general irrep");
+  const int base = ctx->use_sp ? GH_PATH_CLOSED_FORM : GH_PATH_TENSOR;
+  if (path == GH_PATH_PRODUCT) {
+    if (!ctx->has_prod) return fail(ctx, GH_ERR_ARG, "this irrep has no product-of-adjoints form");
+    ctx->b.gen_prod = 1;
+  } else if (path == base) {
+    ctx->b.gen_prod = 0;
+  } else {
+    return fail(ctx, GH_ERR_ARG, "path not available for this context");
+  }
+  invalidate_graph(ctx);
   return GH_OK;
 }
 
@@ -536,7 +576,7 @@ int gh_ctx_create(int D, int N, int n_lat, const int* L, const gh_rep_desc* rep,
     stage = std::max<size_t>(stage, (size_t)V * std::max<size_t>(std::max<size_t>((size_t)D * N * N * 2, (size_t)D * ctx->ng), (size_t)ctx->d * 2));
   }
   ctx->nU = u; ctx->nP = p; ctx->nF = f; ctx->nG = g;
-  std::vector<Work> wg;
+  std::vector<Work> wg, wgp;
   int gw = GEN_WARPS;
   if (ctx->rep == REP_GEN) {
     // one warp per link.  Tensor path: a buffer of N^n complex numbers in shared memory.
@@ -570,6 +610,16 @@ int gh_ctx_create(int D, int N, int n_lat, const int* L, const gh_rep_desc* rep,
       for (int mu = 0; mu < D; ++mu)
         for (int s0 = 0; s0 < ctx->lat_h[l].V; s0 += gw)
           wg.push_back(Work{l, mu, s0, std::min(gw, ctx->lat_h[l].V - s0)});
+    // irreps inside the adjoint product: the product kernel, one item per 32-site block
+    // and direction (taken over the tensor and closed-form paths when available)
+    std::string pwhy;
+    if (rep->W && ghadj::build(N, rep->n_boxes, rep->d, rep->dimT, rep->W, ctx->prod, &pwhy)) {
+      ctx->has_prod = true;
+      for (int l = 0; l < n_lat; ++l)
+        for (int mu = 0; mu < D; ++mu)
+          for (int s0 = 0; s0 < ctx->lat_h[l].V; s0 += GP_LINKS)
+            wgp.push_back(Work{l, mu, s0, std::min(GP_LINKS, ctx->lat_h[l].V - s0)});
+    }
   }
   std::vector<Work> wall = wl;
   wall.insert(wall.end(), ws.begin(), ws.end());
@@ -599,10 +649,12 @@ int gh_ctx_create(int D, int N, int n_lat, const int* L, const gh_rep_desc* rep,
   }
   b.U = U; b.Us = Us; b.P = P; b.phi = phi; b.phis = phis; b.pi = pi; b.psif = psif; b.psib = psib;
   b.nw_links = (int)wl.size(); b.nw_sites = (int)ws.size(); b.nw_gen = (int)wg.size(); b.gen_warps = gw;
+  b.nw_gprod = (int)wgp.size(); b.gen_prod = ctx->has_prod ? 1 : 0;
   b.hist_cap = 1024;
   b.nlat = n_lat; b.D = D; b.N = N; b.d = ctx->d; b.rep = ctx->rep; b.scalar = ctx->scalar; b.st = ctx->st;
   if ((rc = dalloc(ctx, &b.lats, n_lat)) || (rc = dalloc(ctx, &b.w_all, wall.size())) ||
-      (rc = dalloc(ctx, &b.w_gen, std::max<size_t>(wg.size(), 1))) || (rc = dalloc(ctx, &b.blk_first, blk_first.size())) ||
+      (rc = dalloc(ctx, &b.w_gen, std::max<size_t>(wg.size(), 1))) ||
+      (rc = dalloc(ctx, &b.w_gprod, std::max<size_t>(wgp.size(), 1))) || (rc = dalloc(ctx, &b.blk_first, blk_first.size())) ||
       (rc = dalloc(ctx, &b.partials, (size_t)ws.size() * NRED)) || (rc = dalloc(ctx, &b.res, (size_t)n_lat * 2 * NRES)) ||
       (rc = dalloc(ctx, &b.hist, (size_t)n_lat * b.hist_cap)) || (rc = dalloc(ctx, &ctx->staging, stage)) ||
       (rc = dalloc(ctx, &ctx->fbuf, (size_t)std::max<long long>(p, 1))) ||
@@ -612,6 +664,7 @@ int gh_ctx_create(int D, int N, int n_lat, const int* L, const gh_rep_desc* rep,
   CK(cudaMemcpyAsync(b.lats, ctx->lat_h.data(), sizeof(LatDev) * n_lat, cudaMemcpyHostToDevice, ctx->st));
   CK(cudaMemcpyAsync(b.w_all, wall.data(), sizeof(Work) * wall.size(), cudaMemcpyHostToDevice, ctx->st));
   if (!wg.empty()) CK(cudaMemcpyAsync(b.w_gen, wg.data(), sizeof(Work) * wg.size(), cudaMemcpyHostToDevice, ctx->st));
+  if (!wgp.empty()) CK(cudaMemcpyAsync(b.w_gprod, wgp.data(), sizeof(Work) * wgp.size(), cudaMemcpyHostToDevice, ctx->st));
   CK(cudaMemcpyAsync(b.blk_first, blk_first.data(), sizeof(int) * blk_first.size(), cudaMemcpyHostToDevice, ctx->st));
   if ((rc = rebuild_kick_table(ctx))) { g_err = ctx->err; return rc; }
   if (ctx->rep == REP_GEN) {

@@ -31,6 +31,9 @@ struct Bufs {
   int nw_links, nw_sites;
   Work* w_gen;     // general irrep: items of gen_warps links (one warp per link)
   int nw_gen;
+  Work* w_gprod;   // general irrep, product of adjoints: items of up to 32 links (one 32-site block)
+  int nw_gprod;
+  int gen_prod;    // 1: general-irrep link work through k_gen_prod (gen.pq64 set)
   int gen_warps;   // warps per block of k_gen_links (1..GEN_WARPS, from the tensor size)
   int* blk_first;  // [nlat+1] first site item of each lattice (relative to the site items)
   Work* w_kick;    // kick items over 4-D tiles (LatDev::lt): link items then site items
@@ -76,7 +79,13 @@ struct Engine : EngineBase {
   }
   int prepare(const Bufs& b) override {
     if (REP != REP_GEN) return 0;
-    const cudaError_t e = cudaFuncSetAttribute(k_gen_links<D, N, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)gen_smem(b));
+    cudaError_t e = cudaFuncSetAttribute(k_gen_links<D, N, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)gen_smem(b));
+    if (e == cudaSuccess && b.gen.pq64) {
+      e = b.gen.pK == 1 ? cudaFuncSetAttribute(k_gen_prod<D, N, R, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                               (int)gen_prod_smem<N, 1, C>(b.d))
+                        : cudaFuncSetAttribute(k_gen_prod<D, N, R, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                               (int)gen_prod_smem<N, 2, C>(b.d));
+    }
     return e == cudaSuccess ? 0 : -1;
   }
   void kick(const Bufs& b, double eps, int mode, int flags, double* out, bool links, bool sites) override {
@@ -99,6 +108,12 @@ struct Engine : EngineBase {
     a.work = b.w_gen; a.lats = b.lats; a.U = b.U; a.P = b.P; a.phi = b.phi; a.psif = b.psif; a.psib = b.psib;
     a.t = b.gen; a.eps = eps; a.mode = mode; a.out = out;
     a.pot = b.pot; a.sa = b.sa64; a.wpot = b.wpot;
+    if (b.gen_prod && b.gen.pq64 && b.pot != POT_MULTI) {   // the potential's w is computed by k_gen_links
+      a.work = b.w_gprod;
+      if (b.gen.pK == 1) launch(k_gen_prod<D, N, R, 1>, b.nw_gprod, GP_THREADS, gen_prod_smem<N, 1, C>(b.d), b.st, a);
+      else launch(k_gen_prod<D, N, R, 2>, b.nw_gprod, GP_THREADS, gen_prod_smem<N, 2, C>(b.d), b.st, a);
+      return;
+    }
     const size_t sm = gen_smem(b);
     launch(k_gen_links<D, N, R>, b.nw_gen, b.gen_warps * 32, sm, b.st, a);
   }

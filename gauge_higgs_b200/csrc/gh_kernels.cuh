@@ -83,6 +83,10 @@ struct GenTables {                 // general irrep (src/rep/rep_general.hpp), s
   const int* sp_ptr; const double2* sp_c; const unsigned char* sp_e;
   int warp_bytes;                                            // shared memory of one warp
   int px_off;                                                // byte offset of px in a warp's region
+  // irreps inside the K-fold adjoint product (host: gh_adjprod.h): the isometric
+  // intertwiner Q [A][d] in both precisions; null: not available
+  const double2* pq64; const float2* pq32;
+  int pK;
 };
 
 template <typename R> struct V2;
@@ -729,6 +733,190 @@ __global__ void __launch_bounds__(GEN_WARPS * 32) k_gen_links(const GenArgs a) {
     for (int i = 0; i < d; ++i) zim += zc[g * d + i];
     const C F = -(C)L.kappa * (C(-2) * (C)zim);
     const long long pi_ = p_index(L, ng, mu, g, s);
+    if (a.mode == 0) {
+      R* P = (R*)a.P;
+      P[pi_] = (R)((C)P[pi_] - (C)a.eps * F);
+    } else {
+      a.out[pi_] = (double)F;
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// General irreps inside the K-fold adjoint product (K = 1, 2; host set-up and the
+// algebra in gh_adjprod.h): with the fixed isometric intertwiner Q (A x d,
+// A = (N^2 - 1)^K) from the reference's basis into the product,
+//   D_R(U) phi = Q^dag (G (x) ... (x) G) Q phi,   G_ab = 2 Re Tr(T^a U T^b U^dag),
+// and D_R(U)^dag phi with G^T.  One block takes the 32 links of one 32-site block and
+// one direction, 8 threads per link: the lift Q phi and the projection Q^dag y are
+// 64 x 27 and 27 x 64 products shared by the 32 links (every warp reads the same Q
+// entry, every lane its own link); G (x) G acts as X -> G X G^T on each link's 8 x 8
+// coefficient matrix, one row per thread.  Same modes and outputs as k_gen_links
+// (psi_f, psi_b, matter force); the multi-invariant potential's w stays there.
+// The matter force is g^a = -2 Im(phi_x^dag T^a_R psi_f) (src/rep/rep_general.hpp:151-159),
+// one generator per thread, rows summed in order.
+// ---------------------------------------------------------------------------
+constexpr int GP_LINKS = 32;      // links per block (one 32-site block, one direction)
+constexpr int GP_THREADS = 256;   // 8 per link
+template <int N, int K> struct AdjProd {
+  static constexpr int NG = N * N - 1;
+  static constexpr int A = (K == 1) ? NG : NG * NG;
+  static constexpr int RA = (A + 7) / 8;      // rows of A (and of d <= A) per thread
+};
+template <int N, int K, typename C> __host__ __device__ constexpr size_t gen_prod_smem(int d) {
+  return (size_t)(2 * d + AdjProd<N, K>::A) * GP_LINKS * sizeof(cx<C>) +
+         (size_t)AdjProd<N, K>::NG * AdjProd<N, K>::NG * GP_LINKS * sizeof(C);
+}
+
+// out[i] = (D phi)_k, k = q + 8 i, for the link in lane c; Pin: [d][32] input vectors;
+// X: [A][32] work space; G: [NG][NG][32] adjoint matrices.  Every thread of the block calls it.
+template <int N, int K, typename C>
+__device__ __forceinline__ void gp_apply(const typename V2<C>::t* __restrict__ Qv, int d, const cx<C>* Pin, cx<C>* X,
+                                         const C* G, bool dag, int c, int q, cx<C>* out) {
+  constexpr int NG = AdjProd<N, K>::NG, A = AdjProd<N, K>::A, RA = AdjProd<N, K>::RA, LB = GP_LINKS;
+  cx<C> acc[RA];
+#pragma unroll
+  for (int i = 0; i < RA; ++i) acc[i] = zero<C>();
+  for (int l = 0; l < d; ++l) {                         // lift: X = Q phi
+    const cx<C> p = Pin[l * LB + c];
+#pragma unroll
+    for (int i = 0; i < RA; ++i) {
+      const int r = q + 8 * i;
+      if (r < A) {
+        const typename V2<C>::t v = __ldg(Qv + r * d + l);
+        acc[i] = cfma(acc[i], mk<C>(v.x, v.y), p);
+      }
+    }
+  }
+  __syncthreads();                                      // earlier readers of X are done
+#pragma unroll
+  for (int i = 0; i < RA; ++i)
+    if (q + 8 * i < A) X[(q + 8 * i) * LB + c] = acc[i];
+  __syncthreads();
+  auto g = [&](int a, int b) { return dag ? G[(b * NG + a) * LB + c] : G[(a * NG + b) * LB + c]; };
+  if constexpr (K == 1) {                               // y = G x
+    cx<C> y = zero<C>();
+    const int a = q;
+    if (a < NG)
+#pragma unroll
+      for (int k = 0; k < NG; ++k) y = add(y, scale(X[k * LB + c], g(a, k)));
+    __syncthreads();
+    if (a < NG) X[a * LB + c] = y;
+  } else {                                              // Y = G X G^T, row a of this thread
+    const int a = q;
+    cx<C> y[NG];
+    if (a < NG) {
+      cx<C> z[NG];
+#pragma unroll
+      for (int b = 0; b < NG; ++b) {
+        cx<C> sacc = zero<C>();
+#pragma unroll
+        for (int k = 0; k < NG; ++k) sacc = add(sacc, scale(X[(k * NG + b) * LB + c], g(a, k)));
+        z[b] = sacc;
+      }
+#pragma unroll
+      for (int b = 0; b < NG; ++b) {
+        cx<C> sacc = zero<C>();
+#pragma unroll
+        for (int k = 0; k < NG; ++k) sacc = add(sacc, scale(z[k], g(b, k)));
+        y[b] = sacc;
+      }
+    }
+    __syncthreads();
+    if (a < NG)
+#pragma unroll
+      for (int b = 0; b < NG; ++b) X[(a * NG + b) * LB + c] = y[b];
+  }
+  __syncthreads();
+#pragma unroll
+  for (int i = 0; i < RA; ++i) {                        // project: out = Q^dag y
+    const int k = q + 8 * i;
+    cx<C> sacc = zero<C>();
+    if (k < d)
+      for (int r = 0; r < A; ++r) {
+        const typename V2<C>::t v = __ldg(Qv + r * d + k);
+        sacc = cfma_cj(sacc, mk<C>(v.x, v.y), X[r * LB + c]);
+      }
+    out[i] = sacc;
+  }
+}
+
+template <int D, int N, typename R, int K>
+__global__ void __launch_bounds__(GP_THREADS) k_gen_prod(const GenArgs a) {
+  pdl_enter();
+  typedef typename Cmp<R>::t C;
+  constexpr int NG = AdjProd<N, K>::NG, A = AdjProd<N, K>::A, RA = AdjProd<N, K>::RA, LB = GP_LINKS;
+  extern __shared__ unsigned char smem_raw[];
+  const Work w = a.work[blockIdx.x];
+  const LatDev& L = a.lats[w.lat];
+  const int d = a.t.d;
+  const int c = threadIdx.x & (LB - 1), q = threadIdx.x >> 5;
+  cx<C>* Px = reinterpret_cast<cx<C>*>(smem_raw);       // [d][32] phi_x
+  cx<C>* Py = Px + d * LB;                              // [d][32] phi_{x+mu}, then psi_f
+  cx<C>* X = Py + d * LB;                               // [A][32]
+  C* G = reinterpret_cast<C*>(X + A * LB);              // [NG][NG][32]
+  const typename V2<C>::t* Qv =
+      reinterpret_cast<const typename V2<C>::t*>(sizeof(C) == sizeof(double) ? (const void*)a.t.pq64 : (const void*)a.t.pq32);
+  const int mu = w.mu;
+  const bool live = c < w.n;                             // lanes past the lattice's end compute on site s0
+  const int s = w.s0 + (live ? c : 0);
+  int x[D];
+  coords<D>(L, s, x);
+  const int spm = nfwd(L, s, x[mu], mu);
+  const R* phi = (const R*)a.phi;
+  for (int k = q; k < d; k += 8) {
+    Px[k * LB + c] = ldc<C>(phi, f_index(L, d, k, s));
+    Py[k * LB + c] = ldc<C>(phi, f_index(L, d, k, spm));
+  }
+  {
+    const Mat<N, C> U = ld_link<N, C>((const R*)a.U, L, mu, s);
+    for (int b = q; b < NG; b += 8) {                   // column b of G: 2 Tr(T^a U T^b U^dag)
+      C e[NG];
+#pragma unroll
+      for (int k = 0; k < NG; ++k) e[k] = (k == b) ? C(1) : C(0);
+      const Mat<N, C> M = mm_nd(mm(U, alg_to_mat<N, C>(e)), U);
+      cx<C> o[NG];
+      tr2_proj<N, C>(M, o);
+#pragma unroll
+      for (int k = 0; k < NG; ++k) G[(k * NG + b) * LB + c] = o[k].re;
+    }
+  }
+  __syncthreads();
+  R* psif = (R*)a.psif;
+  R* psib = (R*)a.psib;
+  cx<C> o[RA];
+  gp_apply<N, K, C>(Qv, d, Py, X, G, false, c, q, o);  // psi_f = D phi_{x+mu}
+#pragma unroll
+  for (int i = 0; i < RA; ++i) {
+    const int k = q + 8 * i;
+    if (k < d) {
+      Py[k * LB + c] = o[i];
+      if (live) stc<C>(psif, g_index(L, d, mu, k, s), o[i]);
+    }
+  }
+  if (a.mode == 1) return;
+  gp_apply<N, K, C>(Qv, d, Px, X, G, true, c, q, o);   // psi_b = D^dag phi_x
+#pragma unroll
+  for (int i = 0; i < RA; ++i) {
+    const int k = q + 8 * i;
+    if (k < d && live) stc<C>(psib, g_index(L, d, mu, k, s), o[i]);
+  }
+  __syncthreads();
+  for (int gi = q; gi < NG; gi += 8) {                  // matter force, generator gi
+    double zim = 0.0;
+    for (int i = 0; i < d; ++i) {
+      const int r = gi * d + i;
+      cx<C> ti = zero<C>();
+      for (int p = a.t.t_ptr[r]; p < a.t.t_ptr[r + 1]; ++p) {
+        const double2 tv = a.t.t_v[p];
+        ti = cfma(ti, mk<C>((C)tv.x, (C)tv.y), Py[a.t.t_j[p] * LB + c]);
+      }
+      const cx<C> pxi = Px[i * LB + c];
+      zim += (double)pxi.re * (double)ti.im - (double)pxi.im * (double)ti.re;   // Im(conj(phi_i) t_i)
+    }
+    if (!live) continue;
+    const C F = -(C)L.kappa * (C(-2) * (C)zim);
+    const long long pi_ = p_index(L, NG, mu, gi, s);
     if (a.mode == 0) {
       R* P = (R*)a.P;
       P[pi_] = (R)((C)P[pi_] - (C)a.eps * F);

@@ -237,6 +237,8 @@ bool generators(int N, int kind, int d, const double* Tgen, std::vector<cd>& T, 
 
 namespace ghpot {
 
+std::vector<std::complex<double>> gell_mann(int N) { return fund_generators(N); }
+
 int channels(int N, int kind, int d, const double* Tgen, std::vector<double>& c2, std::string& err) {
   if (N != 2 && N != 3) { err = "N must be 2 or 3"; return GH_ERR_UNSUPPORTED; }
   if (d > POT_DMAX) { err = "representation dimension above the potential's limit of " + std::to_string(POT_DMAX); return GH_ERR_UNSUPPORTED; }

@@ -139,6 +139,18 @@ class GeneralRep(Representation):
                                    C.byref(nt)))
         return Dm, nt.value
 
+    def product_matrix(self, U):
+        """D(U) as Q^dag (D_adj(U) (x)...) Q for irreps inside the adjoint's one- or
+        two-fold product (host; gh_rep_product_matrix), with the number of adjoint
+        factors K; raises GaugeHiggsError for irreps outside it."""
+        U = np.ascontiguousarray(U, np.complex128)
+        Dm = np.zeros((self.d, self.d), np.complex128)
+        K = C.c_int()
+        r = self.desc()
+        check(LIB.gh_rep_product_matrix(self.N, C.byref(r), _dptr(U.view(np.float64)), _dptr(Dm.view(np.float64)),
+                                        C.byref(K)))
+        return Dm, K.value
+
     def name(self):
         return "general[" + ",".join(map(str, self.rows)) + "]"
 
@@ -501,12 +513,20 @@ class Ensemble:
                  acc.ctypes.data_as(C.POINTER(C.c_uint64)), _dptr(kap))
         return att, acc, kap
 
+    _PATHS = {0: "register", 1: "tensor", 2: "closed_form", 3: "product"}
+
     def rep_path(self):
         """How the device applies D(U): "register" (fundamental, adjoint), "tensor"
-        (general irreps) or "closed_form" (large single-row irreps)."""
+        (general irreps), "closed_form" (large single-row irreps) or "product" (irreps
+        inside the adjoint's one- or two-fold product, e.g. the SU(3) octet and 27-plet)."""
         p = C.c_int()
         self.ctx("gh_rep_path", C.byref(p))
-        return {0: "register", 1: "tensor", 2: "closed_form"}[p.value]
+        return self._PATHS[p.value]
+
+    def set_rep_path(self, path):
+        """Switch a general irrep between "product" and the path it takes without it."""
+        code = {v: k for k, v in self._PATHS.items()}[path]
+        self.ctx("gh_set_rep_path", code)
 
     def device_bytes(self):
         b = C.c_uint64()

@@ -53,7 +53,7 @@ enum { GH_REP_NONE = 0, GH_REP_FUND = 1, GH_REP_ADJ = 2, GH_REP_GENERAL = 3 };
 enum { GH_PREC_FP64 = 0, GH_PREC_FP32_MD = 1, GH_PREC_FP32_ALL = 2 };
 enum { GH_LEAPFROG = 0, GH_OMELYAN = 1 };
 /* How D(U) of the scalar's representation is applied on the device (gh_rep_path). */
-enum { GH_PATH_REGISTER = 0, GH_PATH_TENSOR = 1, GH_PATH_CLOSED_FORM = 2 };
+enum { GH_PATH_REGISTER = 0, GH_PATH_TENSOR = 1, GH_PATH_CLOSED_FORM = 2, GH_PATH_PRODUCT = 3 };
 
 /* Representation R of the scalar.  Replaces the Representation<N> object
  * (src/rep/representation.hpp:12-32).  GENERAL carries the host-built tables of
@@ -289,6 +289,17 @@ double gh_rng_gauss(uint64_t seed, uint64_t key);
 int gh_rep_general_info(int N, const int* rows, int nrows, int* d, int* n_boxes, long* dimT);
 int gh_rep_general_build(int N, const int* rows, int nrows, double* T, double* W);
 
+/* D(U) of a general irrep as a piece of a product of adjoints (host; no GPU).
+ * For an irrep of n = K N boxes (K = 1, 2; N = 2, 3) the adjoint's K-fold tensor
+ * product holds R: with the fixed isometric intertwiner Q (built from W by the
+ * Levi-Civita embedding of the adjoint into V^(x)N, checked by Schur's lemma and
+ * against the tensor construction), D_R(U) = Q^dag D_adj(U)^(x)K Q, where
+ * D_adj(U)_ab = 2 Re Tr(T^a U T^b U^dag).  The same matrix as the reference's
+ * rep_matrix (src/rep/rep_general.hpp:122-131) to rounding.  U: N x N complex;
+ * D: d x d complex; K (may be NULL) receives the number of adjoint factors.
+ * GH_ERR_REP (message in gh_last_error(NULL)) when the irrep is not reached this way. */
+int gh_rep_product_matrix(int N, const gh_rep_desc* rep, const double* U, double* D, int* K);
+
 /* ---- general irreps: how D(U) is applied ----
  * Fundamental and adjoint: in registers (GH_PATH_REGISTER).  A general irrep uses
  * the exact tensor construction <W_k| U^(x)n |W_l> (GH_PATH_TENSOR;
@@ -302,11 +313,21 @@ int gh_rep_general_build(int N, const int* rows, int nrows, double* T, double* W
  * N^n = 4096); the closed form is the tensor matrix itself, not an approximation
  * of it, and the context checks it against the tensor construction on two test
  * links before using it.
+ * Irreps of n = K N boxes inside the K-fold adjoint product (K = 1, 2; SU(3): the
+ * octet {2,1}, the 27-plet {4,2}, the 10bar {3,3}) take GH_PATH_PRODUCT instead, when
+ * the context finds and checks the intertwiner (gh_rep_product_matrix): a lift by a
+ * fixed A x d matrix shared by 32 links per block, the adjoint matrix of each link
+ * applied K times, a projection -- the reference's tensor matrix to rounding.  The
+ * multi-invariant potential's per-site term is computed on the tensor / closed-form
+ * path, so contexts with that potential use it for their link work.
  * gh_rep_path: the path a context uses.
+ * gh_set_rep_path: switch between GH_PATH_PRODUCT (when available) and the path the
+ *   context would use without it; GH_ERR_ARG for any other path.
  * gh_sympow_matrix: host-only evaluation of the closed form D(U) (U: N x N complex
  *   row-major; D: d x d complex) and the number of terms; GH_ERR_REP when the
  *   irrep has no closed form (message through gh_last_error(NULL)). */
 int gh_rep_path(const gh_ctx* ctx, int* path);
+int gh_set_rep_path(gh_ctx* ctx, int path);
 int gh_sympow_matrix(int N, const gh_rep_desc* rep, const double* U, double* D, long* n_terms);
 
 /* ---- multi-invariant onsite potential ----

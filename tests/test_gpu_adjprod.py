@@ -1,0 +1,93 @@
+"""The product-of-adjoints link kernel (k_gen_prod) against the tensor path and the oracle.
+
+Irreps inside the adjoint's one- or two-fold product (SU(3) octet {2,1}, 27-plet
+{4,2}, 10bar {3,3}; SU(2) {2}, {4}) take GH_PATH_PRODUCT; the same context switched to
+the tensor path must give the same forces, kick and MD evolution (FP64: 1e-12
+relative to the largest entry; FP32-MD: 2e-5), and the oracle's tensor construction
+(src/rep/rep_general.hpp:184-220) the same forces.  Lattices with a volume that is not
+a multiple of 32 exercise the partial last block of every direction.
+"""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def rel_err(a, b):
+    return float(np.abs(np.asarray(a) - np.asarray(b)).max() / max(np.abs(np.asarray(b)).max(), 1e-300))
+
+
+@pytest.mark.parametrize("N,rows,real,path", [(3, [2, 1], True, "product"), (3, [4, 2], True, "product"),
+                                              (3, [3, 3], False, "product"), (3, [2], False, "tensor"),
+                                              (2, [4], False, "product"), (2, [12], False, "closed_form")])
+def test_path_selection(N, rows, real, path):
+    import gauge_higgs_b200 as gh
+    h = gh.GaugeHiggsHMC([4, 4, 4, 4], gh.GeneralRep(N, rows, real=real), seed=1)
+    assert h.rep_path() == path
+    h.close()
+
+
+@pytest.mark.parametrize("precision,tol", [("fp64", 1e-12), ("fp32", 2e-5)])
+@pytest.mark.parametrize("N,rows,real,L", [(3, [4, 2], True, [4, 3, 3, 5]), (3, [2, 1], True, [6, 4, 3, 5]),
+                                           (3, [3, 3], False, [3, 3, 4, 3]), (2, [4], False, [5, 4, 3, 3]),
+                                           (2, [2], False, [4, 4, 4, 4])])
+def test_product_equals_tensor_path(N, rows, real, L, precision, tol):
+    import gauge_higgs_b200 as gh
+    rep = gh.GeneralRep(N, rows, real=real)
+    out = {}
+    for path in ("product", "tensor"):
+        h = gh.GaugeHiggsHMC(L, rep, seed=4, precision=precision, beta=5.7 if N == 3 else 2.3, kappa=0.12, lam=0.5,
+                             nmd=3)
+        if path == "tensor":              # the path the context takes without the product
+            try:
+                h.set_rep_path("tensor")
+            except gh.GaugeHiggsError:
+                h.set_rep_path("closed_form")
+            assert h.rep_path() in ("tensor", "closed_form")
+        else:
+            assert h.rep_path() == "product"
+        h.hot(0.7)
+        h.phi_gaussian(12345, 0.4)
+        f = (h.matter_link_force(), h.scalar_force(), h.measure())
+        h.refresh_momenta()
+        h.md_evolve()
+        out[path] = f + (h.U, h.P, h.pi, h.measure()["H"])
+        h.close()
+    a, b = out["product"], out["tensor"]
+    assert rel_err(a[0], b[0]) < tol
+    assert rel_err(a[1], b[1]) < tol
+    for k in ("S_H", "L_link"):
+        assert abs(a[2][k] - b[2][k]) <= tol * max(1.0, abs(b[2][k]))
+    assert rel_err(a[3], b[3]) < 10 * tol
+    assert rel_err(a[4], b[4]) < 10 * tol
+    assert rel_err(a[5], b[5]) < 10 * tol
+    assert abs(a[6] - b[6]) <= 10 * tol * abs(b[6])
+
+
+@pytest.mark.parametrize("rows,real,L", [([4, 2], True, [3, 3, 2, 5]), ([2, 1], False, [4, 3, 5, 3])])
+def test_product_path_matches_oracle(orc, rows, real, L):
+    import gauge_higgs_b200 as gh
+    from oracle.oracle import REP_GENERAL
+    D, N, kappa, lam = 4, 3, 0.13, 0.5
+    rep = gh.GeneralRep(N, rows, real=real)
+    orep = orc.rep(REP_GENERAL, N, rep.d, int(real), rep.n_boxes, rep.dimT, rep.T, rep.W)
+    U = orc.hot_start(D, N, L, 9, 0.7)
+    phi = orc.phi_gaussian(D, L, rep.d, 9, 12345, int(real), 0.5)
+    h = gh.GaugeHiggsHMC(L, rep, seed=9, beta=5.7, kappa=kappa, lam=lam)
+    assert h.rep_path() == "product"
+    h.U = U
+    h.phi = phi
+    assert rel_err(h.matter_link_force(), orc.matter_force(D, N, L, orep, U, phi, kappa)) < 1e-12
+    assert rel_err(h.scalar_force(), orc.scalar_force(D, N, L, orep, U, phi, kappa, lam)) < 1e-12
+    m = h.measure()
+    assert abs(m["S_H"] - orc.scalar_action(D, N, L, orep, U, phi, kappa, lam)) < 1e-12 * max(1.0, abs(m["S_H"]))
+    h.close()
+
+
+def test_path_switch_rejects_unavailable_paths():
+    import gauge_higgs_b200 as gh
+    from gauge_higgs_b200._lib import GaugeHiggsError
+    h = gh.GaugeHiggsHMC([4, 4, 4, 4], gh.GeneralRep(3, [2]), seed=1)
+    with pytest.raises(GaugeHiggsError):
+        h.set_rep_path("product")
+    h.close()
