@@ -670,8 +670,8 @@ int gh_ctx_create(int D, int N, int n_lat, const int* L, const gh_rep_desc* rep,
   if (ctx->rep == REP_GEN) {
     const size_t sm = ctx->eng->gen_smem(b);
     if (sm > 227 * 1024) { g_err = "general irrep too large for the shared-memory tensor buffer"; return GH_ERR_REP; }
-    if ((rc = ctx->eng->prepare(b))) { g_err = "cudaFuncSetAttribute failed for the general-irrep kernel"; return GH_ERR_CUDA; }
   }
+  if ((rc = ctx->eng->prepare(b))) { g_err = "cudaFuncSetAttribute failed for a kernel of this context"; return GH_ERR_CUDA; }
   // identity links and zero fields as the starting state (GaugeField default is zero
   // matrices; a cold start is the useful default for a device engine)
   InitArgs ia{};
