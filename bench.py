@@ -493,8 +493,21 @@ def run_extra(a, dist):
         ens.hot(0.8)
         ens.phi_gaussian(12345, 0.3)
         ens.enable_tempering(True)
+        sampler = ClockSampler(dist.local)
+        sampler.start()
         v, rec = gpu_rate(ens, 100)
+        clocks = sampler.stop()
         att, acc, _ = ens.tempering_stats()
+        # launch floor: the same trajectory graph (one lattice, same integrator, same launch
+        # count) on a 2^4 lattice, where the kernels have next to no work; its time bounds what
+        # removing launches (one persistent kernel) could save on the C4 ensemble
+        tiny = gh.Ensemble([[2] * 4], gh.FundamentalRep(2), seeds=[1], precision="fp32", beta=2.3, kappa=0.25,
+                           lam=0.5, nmd=20, integ="omelyan")
+        tiny.hot(0.8)
+        tiny.phi_gaussian(12345, 0.3)
+        tiny.enable_tempering(True)
+        v_floor, _ = gpu_rate(tiny, 400)
+        tiny.close()
         sites = sum(L ** 4 for L in Ls) * 16
         cpu = None
         if ref is not None:
@@ -511,7 +524,9 @@ def run_extra(a, dist):
                                 "0.22..0.31, FP32-MD, one graph launch per ensemble trajectory, kappa tempering on",
                     "value": round(v, 2), "unit": "ensemble trajectories/s (64 lattice trajectories each)",
                     "site_updates_per_s": round(v * sites * 20 * 2, 1), "acceptance": float(rec["accepted"].mean()),
-                    "swap_acceptance": float(acc.sum() / max(att.sum(), 1)), "cpu_baseline": cpu})
+                    "swap_acceptance": float(acc.sum() / max(att.sum(), 1)), "cpu_baseline": cpu,
+                    "launch_floor_ms": round(1e3 / v_floor, 4), "ms_per_ensemble_trajectory": round(1e3 / v, 4),
+                    "launch_floor_share": round(v / v_floor, 4), "clocks": clocks})
         ens.close()
     if wl in ("stage0", "all"):
         # the reference's SU(2) -> 2I shakedown point (scripts/su2_stage0.sh: hmc_higgs_multi with

@@ -78,12 +78,6 @@ struct Engine : EngineBase {
     return (size_t)b.gen_warps * b.gen.warp_bytes;
   }
   int prepare(const Bufs& b) override {
-#ifdef GH_KICK_L1_CARVEOUT
-    // shared-memory carveout of the kick (which uses none): GH_KICK_L1_CARVEOUT percent
-    if (cudaFuncSetAttribute(k_kick<D, N, R, REP>, cudaFuncAttributePreferredSharedMemoryCarveout, GH_KICK_L1_CARVEOUT) !=
-        cudaSuccess)
-      return -1;
-#endif
     if (REP != REP_GEN) return 0;
     cudaError_t e = cudaFuncSetAttribute(k_gen_links<D, N, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)gen_smem(b));
     if (e == cudaSuccess && b.gen.pq64) {

@@ -457,9 +457,6 @@ __device__ __forceinline__ void kick_link_dispatch(const KickArgs& a, const LatD
 // FP64: 3 (168 registers).  Measured in the trajectory at SU(3) 16^4 these beat 4 / 2
 // by ~4%: the extra warps hide more of the L2 latency than the spills cost; 6 (80
 // registers) spills too much.
-#ifndef GH_DRIFT_MIX
-#define GH_DRIFT_MIX 0
-#endif
 #ifndef GH_KICK_MINB_F32
 #define GH_KICK_MINB_F32 5
 #endif
@@ -1012,23 +1009,7 @@ __global__ void __launch_bounds__(KBLOCK) k_drift(const DriftArgs a) {
 #pragma unroll
     for (int i = 0; i < N * N; ++i) H.e[i] = scale(H.e[i], (A)a.eps);
     const Mat<N, A> E = expi<N>(H);
-    Mat<N, A> Un;
-#if GH_DRIFT_MIX
-    if constexpr (sizeof(R) < sizeof(A)) {
-      // U' = U + (E - 1) U: the O(eps) correction (E - 1) U as an FP32 product, the sum in FP64
-      Mat<N, R> Em;
-#pragma unroll
-      for (int i = 0; i < N * N; ++i)
-        Em.e[i] = mk<R>((R)(E.e[i].re - ((i % (N + 1)) == 0 ? A(1) : A(0))), (R)E.e[i].im);
-      const Mat<N, R> Uf = ld_link_rw<N, R>((const R*)a.U, L, mu, s);
-      const Mat<N, R> Df = mm(Em, Uf);
-#pragma unroll
-      for (int i = 0; i < N * N; ++i) Un.e[i] = mk<A>((A)Uf.e[i].re + (A)Df.e[i].re, (A)Uf.e[i].im + (A)Df.e[i].im);
-    } else
-#endif
-    {
-      Un = mm(E, ld_link_rw<N, A>((const R*)a.U, L, mu, s));
-    }
+    Mat<N, A> Un = mm(E, ld_link_rw<N, A>((const R*)a.U, L, mu, s));
     if (a.reunit) project_su<N, A>(Un);
     st_link<N, A>((R*)a.U, L, mu, s, Un);
   } else if (a.frozen) {
