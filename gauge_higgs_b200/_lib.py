@@ -53,6 +53,12 @@ _u64p = C.POINTER(C.c_uint64)
 _ctx = C.c_void_p
 
 SIGNATURES = {
+    "gh_set_domain": [_ctx, C.c_int, _ip, _ip, _ip, _ip],
+    "gh_halo_count": [_ctx, C.c_int, C.c_int, C.c_int, C.POINTER(C.c_longlong)],
+    "gh_halo_pack": [_ctx, C.c_int, C.c_int, C.c_int, C.c_int, C.c_void_p],
+    "gh_halo_unpack": [_ctx, C.c_int, C.c_int, C.c_int, C.c_int, C.c_void_p],
+    "gh_save_fields": [_ctx],
+    "gh_restore_fields": [_ctx],
     "gh_set_rep_path": [_ctx, C.c_int],
     "gh_rep_product_matrix": [C.c_int, C.POINTER(RepDesc), _dp, _dp, _ip],
     "gh_ctx_create": [C.c_int, C.c_int, C.c_int, _ip, C.POINTER(RepDesc), C.c_int, _u64p, C.POINTER(C.c_void_p)],

@@ -241,7 +241,16 @@ void enq_trajectory(gh_ctx* ctx) {
   }
 }
 
+bool any_decomposed(const gh_ctx* ctx) {
+  for (const LatDev& L : ctx->lat_h)
+    if (L.dec) return true;
+  return false;
+}
+
 int run_traj(gh_ctx* ctx) {
+  if (any_decomposed(ctx))
+    return fail(ctx, GH_ERR_STATE, "a subdomain of a decomposed lattice: its trajectory is driven by the domain "
+                                   "layer (global dH and accept), not by the device Metropolis");
   if (ctx->use_graph) {
     if (!ctx->gexec) {
       CK(cudaStreamBeginCapture(ctx->st, cudaStreamCaptureModeThreadLocal));
@@ -512,6 +521,97 @@ int gh_set_rep_path(gh_ctx* ctx, int path) {
   return GH_OK;
 }
 
+// ---- domain decomposition (src/mpi/gauge_mpi.hpp, src/mpi/higgs_mpi.hpp) ----
+int gh_set_domain(gh_ctx* ctx, int lat, const int* G, const int* lo, const int* hi, const int* goff) {
+  int rc = check_lat(ctx, lat, false);
+  if (rc) return rc;
+  if (!G || !lo || !hi || !goff) return fail(ctx, GH_ERR_ARG, "null argument");
+  LatDev& L = ctx->lat_h[lat];
+  long long Vi = 1, gs = 1;
+  int dec = 0;
+  for (int mu = 0; mu < ctx->D; ++mu) {
+    const int Lm = L.L[mu];
+    if (G[mu] < 1 || goff[mu] < 0) return fail(ctx, GH_ERR_ARG, "global extents must be >= 1 and offsets >= 0");
+    if (lo[mu] == 0) {
+      // a direction that is not split: the whole periodic extent, no halo
+      if (hi[mu] != Lm || G[mu] != Lm || goff[mu] != 0)
+        return fail(ctx, GH_ERR_ARG, "a direction without halo must hold the whole global extent");
+    } else if (lo[mu] == 1) {
+      // a split direction: interior [1, L-1) between one halo layer on each side
+      if (hi[mu] != Lm - 1 || Lm < 3) return fail(ctx, GH_ERR_ARG, "a split direction needs hi = L - 1 and L >= 3");
+      if (goff[mu] + (hi[mu] - lo[mu]) > G[mu]) return fail(ctx, GH_ERR_ARG, "subdomain reaches past the global extent");
+      dec = 1;
+    } else {
+      return fail(ctx, GH_ERR_ARG, "lo must be 0 (whole direction) or 1 (one halo layer)");
+    }
+    Vi *= hi[mu] - lo[mu];
+  }
+  for (int mu = 0; mu < 4; ++mu) {
+    L.lo[mu] = mu < ctx->D ? lo[mu] : 0;
+    L.hi[mu] = mu < ctx->D ? hi[mu] : 1;
+    L.goff[mu] = mu < ctx->D ? goff[mu] : 0;
+    L.gstr[mu] = gs;
+    gs *= mu < ctx->D ? G[mu] : 1;
+  }
+  L.Vi = (int)Vi;
+  L.dec = dec;
+  // the domain fields close the descriptor: one copy from lo to the end
+  const size_t off = offsetof(LatDev, lo);
+  CK(cudaMemcpyAsync((char*)(ctx->b.lats + lat) + off, (const char*)&L + off, sizeof(LatDev) - off,
+                     cudaMemcpyHostToDevice, ctx->st));
+  CK(cudaStreamSynchronize(ctx->st));
+  invalidate_graph(ctx);
+  return GH_OK;
+}
+
+int gh_halo_count(gh_ctx* ctx, int lat, int field, int nu, long long* n_complex) {
+  int rc = check_lat(ctx, lat, false);
+  if (rc) return rc;
+  if (!n_complex) return fail(ctx, GH_ERR_ARG, "null output");
+  if (nu < 0 || nu >= ctx->D) return fail(ctx, GH_ERR_ARG, "direction out of range");
+  if (field != 0 && !(field == 1 && ctx->scalar)) return fail(ctx, GH_ERR_ARG, "field must be 0 (links) or 1 (phi)");
+  const LatDev& L = ctx->lat_h[lat];
+  const long long nplane = (long long)L.V / L.L[nu];
+  *n_complex = nplane * (field == 0 ? (long long)ctx->D * ctx->N * ctx->N : ctx->d);
+  return GH_OK;
+}
+
+static int halo_op(gh_ctx* ctx, int lat, int field, int nu, int layer, void* buf, int unpack) {
+  long long n = 0;
+  int rc = gh_halo_count(ctx, lat, field, nu, &n);
+  if (rc) return rc;
+  const LatDev& L = ctx->lat_h[lat];
+  if (!buf) return fail(ctx, GH_ERR_ARG, "null buffer");
+  if (layer < 0 || layer >= L.L[nu]) return fail(ctx, GH_ERR_ARG, "layer out of range");
+  if ((reinterpret_cast<uintptr_t>(buf) & 15u) != 0) return fail(ctx, GH_ERR_ARG, "halo buffer must be 16-byte aligned");
+  HaloArgs a{};
+  a.lat = lat; a.f = field == 0 ? ctx->b.U : ctx->b.phi; a.buf = buf; a.kind = field; a.nu = nu; a.layer = layer;
+  a.unpack = unpack; a.D = ctx->D; a.nn = ctx->N * ctx->N; a.d = ctx->d;
+  a.nplane = (long long)L.V / L.L[nu];
+  a.ncomp = field == 0 ? ctx->D * ctx->N * ctx->N : ctx->d;
+  ctx->eng->halo(ctx->b, a);
+  return launch_check(ctx, unpack ? "halo unpack" : "halo pack");
+}
+int gh_halo_pack(gh_ctx* ctx, int lat, int field, int nu, int layer, void* buf) {
+  return halo_op(ctx, lat, field, nu, layer, buf, 0);
+}
+int gh_halo_unpack(gh_ctx* ctx, int lat, int field, int nu, int layer, const void* buf) {
+  return halo_op(ctx, lat, field, nu, layer, const_cast<void*>(buf), 1);
+}
+
+int gh_save_fields(gh_ctx* ctx) {
+  if (!ctx) return fail(nullptr, GH_ERR_ARG, "null context");
+  CK(cudaMemcpyAsync(ctx->b.Us, ctx->b.U, (size_t)ctx->nU * 2 * ctx->rs, cudaMemcpyDeviceToDevice, ctx->st));
+  if (ctx->scalar) CK(cudaMemcpyAsync(ctx->b.phis, ctx->b.phi, (size_t)ctx->nF * 2 * ctx->rs, cudaMemcpyDeviceToDevice, ctx->st));
+  return GH_OK;
+}
+int gh_restore_fields(gh_ctx* ctx) {
+  if (!ctx) return fail(nullptr, GH_ERR_ARG, "null context");
+  CK(cudaMemcpyAsync(ctx->b.U, ctx->b.Us, (size_t)ctx->nU * 2 * ctx->rs, cudaMemcpyDeviceToDevice, ctx->st));
+  if (ctx->scalar) CK(cudaMemcpyAsync(ctx->b.phi, ctx->b.phis, (size_t)ctx->nF * 2 * ctx->rs, cudaMemcpyDeviceToDevice, ctx->st));
+  return GH_OK;
+}
+
 uint64_t gh_rng_key(uint64_t a, uint64_t b, uint64_t c, uint64_t d, uint64_t e) { return ghrng::key(a, b, c, d, e); }
 double gh_rng_uniform(uint64_t seed, uint64_t key) { return ghrng::uniform(seed, key); }
 double gh_rng_gauss(uint64_t seed, uint64_t key) { return ghrng::gauss(seed, key); }
@@ -561,6 +661,9 @@ int gh_ctx_create(int D, int N, int n_lat, const int* L, const gh_rep_desc* rep,
     }
     if ((V + ULANE) * D * N * N > (1LL << 31) - 1) return fail(nullptr, GH_ERR_ARG, "lattice too large for 32-bit site indexing");
     Ld.V = (int)V; Ld.Vp = (int)((V + ULANE - 1) / ULANE * ULANE); Ld.cidx = l;
+    // the whole lattice is active: no halo, global site = local site
+    for (int mu = 0; mu < 4; ++mu) { Ld.lo[mu] = 0; Ld.hi[mu] = Ld.L[mu]; Ld.goff[mu] = 0; Ld.gstr[mu] = Ld.stride[mu]; }
+    Ld.Vi = (int)V; Ld.dec = 0;
     Ld.u_off = u; Ld.p_off = p; Ld.f_off = f; Ld.g_off = g;
     Ld.beta = 2.3; Ld.kappa = 0.1; Ld.lambda = 0.5; Ld.seed = seeds[l];
     for (int mu = 0; mu < D; ++mu)
@@ -967,6 +1070,7 @@ int probe_rep(gh_ctx* ctx, const int* rows, int nrows, LoopArgs& a, double& d) {
 // mu < nu (wilson_loop_fund / wilson_loop_rep, src/measure/observables.hpp:48-79);
 // Polyakov loops traced in a probe irrep (polyakov_loop_rep, :81-101).
 int gh_wilson_loop(gh_ctx* ctx, int lat, int Ra, int Rb, const int* rows, int nrows, double* out) {
+  if (ctx && any_decomposed(ctx)) return fail(ctx, GH_ERR_UNSUPPORTED, "not available on a subdomain of a decomposed lattice");
   int rc = check_lat(ctx, lat, true);
   if (rc) return rc;
   if (!out) return fail(ctx, GH_ERR_ARG, "null output");
@@ -983,6 +1087,7 @@ int gh_wilson_loop(gh_ctx* ctx, int lat, int Ra, int Rb, const int* rows, int nr
 }
 
 int gh_polyakov_rep(gh_ctx* ctx, int lat, int tdir, const int* rows, int nrows, double* out) {
+  if (ctx && any_decomposed(ctx)) return fail(ctx, GH_ERR_UNSUPPORTED, "not available on a subdomain of a decomposed lattice");
   int rc = check_lat(ctx, lat, true);
   if (rc) return rc;
   if (!out) return fail(ctx, GH_ERR_ARG, "null output");
@@ -1000,6 +1105,7 @@ int gh_polyakov_rep(gh_ctx* ctx, int lat, int tdir, const int* rows, int nrows, 
 }
 
 int gh_polyakov(gh_ctx* ctx, int lat, int tdir, double* out) {
+  if (ctx && any_decomposed(ctx)) return fail(ctx, GH_ERR_UNSUPPORTED, "not available on a subdomain of a decomposed lattice");
   int rc = check_lat(ctx, lat, true);
   if (rc) return rc;
   if (!out) return fail(ctx, GH_ERR_ARG, "null output");
@@ -1275,6 +1381,7 @@ int gh_trajectory_host(gh_ctx* ctx, double* U, double* phi, gh_traj_record* rec)
 }
 
 int gh_temper_enable(gh_ctx* ctx, int mode, uint64_t swap_seed) {
+  if (ctx && any_decomposed(ctx)) return fail(ctx, GH_ERR_UNSUPPORTED, "not available on a subdomain of a decomposed lattice");
   if (!ctx) return fail(nullptr, GH_ERR_ARG, "null context");
   invalidate_graph(ctx);
   if (mode == 0) { ctx->temper = 0; return GH_OK; }

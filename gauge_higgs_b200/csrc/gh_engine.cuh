@@ -2,6 +2,7 @@
 // The context (gh_ctx.cu) holds one Engine chosen at creation; every launch goes
 // to the context's stream, so a whole trajectory can be captured as a graph.
 #pragma once
+#include <algorithm>
 #include "gh_kernels.cuh"
 
 namespace ghk {
@@ -66,6 +67,7 @@ struct EngineBase {
   virtual void polyakov(const Bufs& b, int tdir) = 0;
   virtual void loops(const Bufs& b, LoopArgs a) = 0;
   virtual void xfer(const Bufs& b, XferArgs a) = 0;
+  virtual void halo(const Bufs& b, HaloArgs a) = 0;
   virtual size_t gen_smem(const Bufs& b) const = 0;
   virtual int prepare(const Bufs& b) = 0;
 };
@@ -170,6 +172,12 @@ struct Engine : EngineBase {
   void xfer(const Bufs& b, XferArgs a) override {
     a.lats = b.lats;
     k_xfer<R><<<296, 256, 0, b.st>>>(a);
+  }
+  void halo(const Bufs& b, HaloArgs a) override {
+    a.lats = b.lats;
+    const long long total = a.nplane * a.ncomp;
+    const unsigned grid = (unsigned)std::min<long long>((total + 255) / 256, 148 * 8);
+    if (grid) k_halo<R><<<grid, 256, 0, b.st>>>(a);
   }
 };
 

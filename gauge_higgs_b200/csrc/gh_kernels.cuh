@@ -64,7 +64,48 @@ struct LatDev {
   unsigned long long traj, accepted, nonfinite;
   int last_acc;
   int lt[4];                     // kick tile shape: log2 of the tile extent per direction
+  // Domain decomposition (src/mpi/gauge_mpi.hpp:26-80): a subdomain is stored with a
+  // width-1 halo in every split direction.  Kernels act on the active box [lo, hi) only
+  // (the whole lattice when not decomposed), and the counter RNG is keyed on the global
+  // site index sum_mu (x_mu - lo_mu + goff_mu) * gstr_mu, so a decomposed lattice draws
+  // the same numbers as the whole one.
+  int lo[4], hi[4];
+  int goff[4];
+  long long gstr[4];
+  int Vi;                        // active sites (normalises the lattice's sums)
+  int dec;                       // 1: a subdomain with halo sites
 };
+// Site s inside the active box (always true for a lattice that is not decomposed).
+__device__ __forceinline__ bool active_site(const LatDev& L, int s) {
+  if (!L.dec) return true;
+  int r = s;
+#pragma unroll
+  for (int mu = 0; mu < 4; ++mu) {
+    const int x = r % L.L[mu];
+    r /= L.L[mu];
+    if (x < L.lo[mu] || x >= L.hi[mu]) return false;
+  }
+  return true;
+}
+template <int D> __device__ __forceinline__ bool in_box(const LatDev& L, const int* x) {
+  bool in = true;
+#pragma unroll
+  for (int mu = 0; mu < D; ++mu) in = in && (x[mu] >= L.lo[mu]) && (x[mu] < L.hi[mu]);
+  return in;
+}
+// Global site index of local site s (the RNG key's site).
+__device__ __forceinline__ long long global_site(const LatDev& L, int s) {
+  if (!L.dec) return s;
+  long long g = 0;
+  int r = s;
+#pragma unroll
+  for (int mu = 0; mu < 4; ++mu) {
+    const int x = r % L.L[mu];
+    r /= L.L[mu];
+    g += (long long)(x - L.lo[mu] + L.goff[mu]) * L.gstr[mu];
+  }
+  return g;
+}
 // Block work item.  Linear items: sites s0 .. s0+n-1.  Kick items (tiles): s0 is
 // the tile's origin site and n packs the origin coordinates, 8 bits each.
 // mu = -1 marks a site item, mu >= 0 a link item of direction mu.
@@ -165,7 +206,7 @@ __device__ __forceinline__ int nbwd(const LatDev& L, int s, int xm, int mu) {
 }
 // Site of thread `tid` inside a kick tile: the tile's origin comes from the work
 // item, the offset from tid split by the power-of-two tile extents.  Threads that
-// fall outside the lattice (partial tiles) return false.
+// fall outside the lattice's active box (partial tiles, halo sites) return false.
 template <int D>
 __device__ __forceinline__ bool tile_site(const LatDev& L, const Work& w, int tid, int& s, int* x) {
   s = w.s0;
@@ -176,7 +217,7 @@ __device__ __forceinline__ bool tile_site(const LatDev& L, const Work& w, int ti
     const int l = r & ((1 << L.lt[mu]) - 1);
     r >>= L.lt[mu];
     x[mu] = ((w.n >> (8 * mu)) & 0xFF) + l;
-    in = in && (x[mu] < L.L[mu]);
+    in = in && (x[mu] >= L.lo[mu]) && (x[mu] < L.hi[mu]);
     s += l * L.stride[mu];
   }
   return in && (r == 0);
@@ -648,6 +689,7 @@ __global__ void __launch_bounds__(GEN_WARPS * 32) k_gen_links(const GenArgs a) {
   const R* phi = (const R*)a.phi;
   int x[D];
   coords<D>(L, s, x);
+  if (!in_box<D>(L, x)) return;                  // halo link of a subdomain (whole warp)
   const int spm = nfwd(L, s, x[mu], mu);
   const Mat<N, C> M = ld_link<N, C>(U, L, mu, s);
   for (int k = lane; k < d; k += 32) {
@@ -858,10 +900,10 @@ __global__ void __launch_bounds__(GP_THREADS) k_gen_prod(const GenArgs a) {
   const typename V2<C>::t* Qv =
       reinterpret_cast<const typename V2<C>::t*>(sizeof(C) == sizeof(double) ? (const void*)a.t.pq64 : (const void*)a.t.pq32);
   const int mu = w.mu;
-  const bool live = c < w.n;                             // lanes past the lattice's end compute on site s0
-  const int s = w.s0 + (live ? c : 0);
+  const int s = w.s0 + (c < w.n ? c : 0);              // lanes past the lattice's end compute on site s0
   int x[D];
   coords<D>(L, s, x);
+  const bool live = c < w.n && in_box<D>(L, x);        // and store nothing, as halo sites of a subdomain
   const int spm = nfwd(L, s, x[mu], mu);
   const R* phi = (const R*)a.phi;
   for (int k = q; k < d; k += 8) {
@@ -997,6 +1039,7 @@ __global__ void __launch_bounds__(KBLOCK) k_drift(const DriftArgs a) {
   if ((int)threadIdx.x >= w.n) return;
   const LatDev L = a.lats[w.lat];
   const int s = w.s0 + threadIdx.x;
+  if (!active_site(L, s)) return;
   if (w.mu >= 0) {
     const int mu = w.mu;
     constexpr int ng = N * N - 1;
@@ -1068,6 +1111,7 @@ __global__ void __launch_bounds__(KBLOCK) k_sphere(const SphereArgs a) {
   if ((int)threadIdx.x >= w.n) return;
   const LatDev& L = a.lats[w.lat];
   const int s = w.s0 + threadIdx.x;
+  if (!active_site(L, s)) return;
   R* phi = (R*)a.phi;
   R* pi = (R*)a.pi;
   if (a.what == 0) {
@@ -1102,6 +1146,7 @@ __global__ void __launch_bounds__(KBLOCK) k_reunit(const LinkArgs a) {
   if ((int)threadIdx.x >= w.n || w.mu < 0) return;
   const LatDev L = a.lats[w.lat];
   const int s = w.s0 + threadIdx.x;
+  if (!active_site(L, s)) return;
   Mat<N, double> M = ld_link_rw<N, double>((const R*)a.U, L, w.mu, s);
   reunitarize<N, double>(M);
   st_link<N, double>((R*)a.U, L, w.mu, s, M);
@@ -1144,7 +1189,7 @@ __global__ void __launch_bounds__(KBLOCK) k_measure(const MeasArgs a) {
   pdl_enter();
   const Work w = a.work[blockIdx.x];
   double r[NRED] = {0, 0, 0, 0, 0, 0};
-  if ((int)threadIdx.x < w.n) {
+  if ((int)threadIdx.x < w.n && active_site(a.lats[w.lat], w.s0 + (int)threadIdx.x)) {
     const LatDev L = a.lats[w.lat];
     const int s = w.s0 + threadIdx.x;
     const R* U = (const R*)a.U;
@@ -1271,7 +1316,7 @@ static __global__ void k_finalize(const FinArgs a) {
 #pragma unroll
     for (int k = 0; k < NRED; ++k) { t[k] = 0.0; for (int q = 0; q < 32; ++q) t[k] += sh[k][q]; }
     const LatDev L = a.lats[l];
-    const double Vd = (double)L.V;
+    const double Vd = (double)L.Vi;              // active sites (all of a lattice that is not decomposed)
     const double nplaq = Vd * (a.D * (a.D - 1) / 2);
     const double Sg = (L.beta / a.N) * ((double)a.N * nplaq - t[0]);
     const double SH = a.scalar ? (t[1] - 2.0 * L.kappa * t[2]) : 0.0;
@@ -1349,6 +1394,46 @@ __global__ void __launch_bounds__(KBLOCK) k_restore(const RestoreArgs a) {
 }
 
 // ---------------------------------------------------------------------------
+// Halo planes of a subdomain (src/mpi/gauge_mpi.hpp:101-139): gather (pack) or scatter
+// (unpack) every site of the local lattice with x_nu = layer, all components of the
+// links (kind 0: D N^2 complex per site) or of phi (kind 1: d complex per site), to or
+// from a contiguous buffer [component][plane site], the plane's sites in mixed radix
+// over the other directions, direction 0 fastest.  Whole planes, halo sites of the other
+// directions included, so that exchanging the split directions one after the other
+// also fills the edges and corners, as the reference's sequential exchange does.
+// ---------------------------------------------------------------------------
+struct HaloArgs {
+  const LatDev* lats;
+  int lat;
+  void* f;              // the field (U or phi)
+  void* buf;            // device buffer, ncomp * nplane complex R
+  int kind, nu, layer, unpack, D, nn, d;
+  long long nplane;
+  int ncomp;
+};
+template <typename R>
+__global__ void __launch_bounds__(256) k_halo(const HaloArgs a) {
+  typedef typename V2<R>::t V;
+  const LatDev& L = a.lats[a.lat];
+  const long long total = a.nplane * a.ncomp;
+  V* f = reinterpret_cast<V*>(a.f);
+  V* b = reinterpret_cast<V*>(a.buf);
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (long long)gridDim.x * blockDim.x) {
+    const int comp = (int)(i / a.nplane);
+    long long r = i - (long long)comp * a.nplane;
+    int s = a.layer * L.stride[a.nu];
+    for (int mu = 0; mu < a.D; ++mu) {
+      if (mu == a.nu) continue;
+      s += (int)(r % L.L[mu]) * L.stride[mu];
+      r /= L.L[mu];
+    }
+    const long long e = a.kind == 0 ? u_index(L, a.nn, comp / a.nn, comp % a.nn, s) : f_index(L, a.d, comp, s);
+    if (a.unpack) f[e] = b[i];
+    else b[i] = f[e];
+  }
+}
+
+// ---------------------------------------------------------------------------
 // Counter-RNG field initialisation (bit-exact keys of the reference):
 //   hot start  U = expi(alg_to_mat(sigma * gauss(key(1, s, mu, a))))  src/core/fields.hpp:25-34
 //   momenta    P^a = gauss(key(stream, s, mu, a))                       src/core/fields.hpp:59-66
@@ -1385,6 +1470,8 @@ __global__ void __launch_bounds__(KBLOCK) k_init(const InitArgs a) {
   if ((int)threadIdx.x >= w.n) return;
   const LatDev L = a.lats[w.lat];
   const int s = w.s0 + threadIdx.x;
+  if (!active_site(L, s)) return;                 // halo sites come from the neighbours
+  const long long gs = global_site(L, s);         // the RNG key's site
   constexpr int ng = N * N - 1;
   if (w.mu >= 0) {
     const int mu = w.mu;
@@ -1393,7 +1480,7 @@ __global__ void __launch_bounds__(KBLOCK) k_init(const InitArgs a) {
       if (a.what == 0) {
         double v[ng];
 #pragma unroll
-        for (int g = 0; g < ng; ++g) v[g] = a.sigma * ghrng::gauss(L.seed, ghrng::key(1, s, mu, g));
+        for (int g = 0; g < ng; ++g) v[g] = a.sigma * ghrng::gauss(L.seed, ghrng::key(1, gs, mu, g));
         M = expi<N>(alg_to_mat<N, double>(v));
       } else {
         set_ident(M);
@@ -1404,7 +1491,7 @@ __global__ void __launch_bounds__(KBLOCK) k_init(const InitArgs a) {
       R* P = (R*)a.P;
       const long long pb = p_index(L, ng, mu, 0, s);
 #pragma unroll
-      for (int g = 0; g < ng; ++g) P[pb + g * ULANE] = (R)gauss_r<R>(L.seed, ghrng::key(st, s, mu, g));
+      for (int g = 0; g < ng; ++g) P[pb + g * ULANE] = (R)gauss_r<R>(L.seed, ghrng::key(st, gs, mu, g));
     }
     return;
   }
@@ -1415,8 +1502,8 @@ __global__ void __launch_bounds__(KBLOCK) k_init(const InitArgs a) {
     const double sg = (a.what == 1) ? 1.0 : a.sigma;
     R* vec = (R*)a.vec;
     for (int k = 0; k < a.d; ++k) {
-      const double re = sg * gauss_r<R>(L.seed, ghrng::key(st, s, 2 * k));
-      const double im = a.real ? 0.0 : sg * gauss_r<R>(L.seed, ghrng::key(st, s, 2 * k + 1));
+      const double re = sg * gauss_r<R>(L.seed, ghrng::key(st, gs, 2 * k));
+      const double im = a.real ? 0.0 : sg * gauss_r<R>(L.seed, ghrng::key(st, gs, 2 * k + 1));
       stc<double>(vec, f_index(L, a.d, k, s), mk<double>(re, im));
     }
   } else if (a.what == 5) {

@@ -274,6 +274,36 @@ const char* gh_mlp_last_error(void);
 int gh_plaquette_noalloc(int D, int N, const int* L, const double* U_dev, double* out_dev, void* stream);
 const char* gh_noalloc_last_error(void);
 
+/* ---- domain decomposition (src/mpi/gauge_mpi.hpp:26-139, src/mpi/higgs_mpi.hpp:150-226) ----
+ * A lattice too large for one GPU is split over a process grid; each rank's context
+ * holds its subdomain padded by a width-1 halo in every split direction (local
+ * extent = interior + 2) and the whole extent in the others.  The reference's
+ * DistLattice / DistGaugeHiggsHMC with MPI_Sendrecv halos; here the host moves the
+ * halo planes (NCCL or any transport) between these calls:
+ * gh_set_domain: G the global extents; per direction lo = 0, hi = L (not split) or
+ *   lo = 1, hi = L - 1 (split); goff the global coordinate of the local coordinate lo.
+ *   Kernels then act on the interior only, the counter RNG is keyed on the global site
+ *   index (hot start, phi init and heatbaths equal the whole lattice's draws), and
+ *   gh_measure's sums cover the interior (normalised by its volume: H, S_g, S_H and
+ *   the kinetic terms add over ranks, the averages combine weighted by volume).  The
+ *   device Metropolis, tempering and loop observables are refused on a subdomain: the
+ *   host takes the global dH and the accept decision (the same key on every rank).
+ * gh_halo_count: complex elements of one plane x_nu = const of field 0 (links, D N^2
+ *   per site) or 1 (phi, d per site), whole padded plane.
+ * gh_halo_pack / gh_halo_unpack: gather / scatter that plane at x_nu = layer to / from
+ *   a device buffer (16-byte aligned, field precision, [component][plane site] with
+ *   the plane's sites in mixed radix over the other directions, direction 0 fastest).
+ *   Exchanging the split directions in order with whole planes also fills edges and
+ *   corners (the reference's sequential halo_exchange_raw).
+ * gh_save_fields / gh_restore_fields: copy U and phi to / from the context's
+ *   trajectory save buffers (the reject branch of trajectory()). */
+int gh_set_domain(gh_ctx* ctx, int lat, const int* G, const int* lo, const int* hi, const int* goff);
+int gh_halo_count(gh_ctx* ctx, int lat, int field, int nu, long long* n_complex);
+int gh_halo_pack(gh_ctx* ctx, int lat, int field, int nu, int layer, void* buf);
+int gh_halo_unpack(gh_ctx* ctx, int lat, int field, int nu, int layer, const void* buf);
+int gh_save_fields(gh_ctx* ctx);
+int gh_restore_fields(gh_ctx* ctx);
+
 /* ---- the counter RNG on the host (src/core/rng.hpp:11-46) ----
  * Same bits as the device kernels: key and uniform are integer exact; gauss is the
  * correctly rounded evaluation of sqrt(-2 log u1) cos(2 pi u2).  Pure functions
