@@ -87,6 +87,15 @@ __device__ __forceinline__ bool active_site(const LatDev& L, int s) {
   }
   return true;
 }
+// Below the active box's upper end in every direction: the interior and the lower halo
+// layer, where the general-irrep link kernels also write psi_b = D(U)^dag phi, which the
+// scalar force of the first interior layer reads at x - mu.
+template <int D> __device__ __forceinline__ bool below_hi(const LatDev& L, const int* x) {
+  bool in = true;
+#pragma unroll
+  for (int mu = 0; mu < D; ++mu) in = in && (x[mu] < L.hi[mu]);
+  return in;
+}
 template <int D> __device__ __forceinline__ bool in_box(const LatDev& L, const int* x) {
   bool in = true;
 #pragma unroll
@@ -689,7 +698,8 @@ __global__ void __launch_bounds__(GEN_WARPS * 32) k_gen_links(const GenArgs a) {
   const R* phi = (const R*)a.phi;
   int x[D];
   coords<D>(L, s, x);
-  if (!in_box<D>(L, x)) return;                  // halo link of a subdomain (whole warp)
+  if (!below_hi<D>(L, x)) return;                // upper halo link of a subdomain (whole warp)
+  const bool own = in_box<D>(L, x);              // the link's momentum belongs to this subdomain
   const int spm = nfwd(L, s, x[mu], mu);
   const Mat<N, C> M = ld_link<N, C>(U, L, mu, s);
   for (int k = lane; k < d; k += 32) {
@@ -755,7 +765,7 @@ __global__ void __launch_bounds__(GEN_WARPS * 32) k_gen_links(const GenArgs a) {
     stc<C>(psif, gi, pf[k]);
     if (a.mode != 1) stc<C>(psib, gi, pb[k]);
   }
-  if (a.mode == 1) return;
+  if (a.mode == 1 || !own) return;
   // matter force: g^a = -2 Im(phi_x^dag T^a_R psi_f), F^a = -kappa g^a.  The lanes
   // split the (a, row) pairs; the rows of each a are then summed in order.
   constexpr int ng = N * N - 1;
@@ -903,7 +913,8 @@ __global__ void __launch_bounds__(GP_THREADS) k_gen_prod(const GenArgs a) {
   const int s = w.s0 + (c < w.n ? c : 0);              // lanes past the lattice's end compute on site s0
   int x[D];
   coords<D>(L, s, x);
-  const bool live = c < w.n && in_box<D>(L, x);        // and store nothing, as halo sites of a subdomain
+  const bool live = c < w.n && below_hi<D>(L, x);      // and store nothing, as upper halo sites of a subdomain
+  const bool own = live && in_box<D>(L, x);            // momentum updates: interior links only
   const int spm = nfwd(L, s, x[mu], mu);
   const R* phi = (const R*)a.phi;
   for (int k = q; k < d; k += 8) {
@@ -956,7 +967,7 @@ __global__ void __launch_bounds__(GP_THREADS) k_gen_prod(const GenArgs a) {
       const cx<C> pxi = Px[i * LB + c];
       zim += (double)pxi.re * (double)ti.im - (double)pxi.im * (double)ti.re;   // Im(conj(phi_i) t_i)
     }
-    if (!live) continue;
+    if (!own) continue;
     const C F = -(C)L.kappa * (C(-2) * (C)zim);
     const long long pi_ = p_index(L, NG, mu, gi, s);
     if (a.mode == 0) {

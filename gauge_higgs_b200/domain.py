@@ -341,8 +341,10 @@ class DomainHMC:
         self._dirty = True
         Hi = self.hamiltonian()
         self.md_evolve()
-        for h in self.h:
-            h.reunitarize_all()
+        if self.h[0].precision == "fp64":
+            # the reference's end-of-trajectory reunitarisation; FP32-MD projects in every drift
+            for h in self.h:
+                h.reunitarize_all()
         self._dirty = True
         Hf = self.hamiltonian()
         self.last_dH = Hf - Hi

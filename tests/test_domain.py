@@ -111,3 +111,11 @@ def test_gloo_ranks_exchange_halos(G, P):
     assert all(o[1] == "ok" for o in out), out
     want = sum(r + 0.25 for r in range(world))
     assert all(o[2] == want for o in out)          # every rank holds the same sum
+
+
+def test_mpi_driver_argument_errors():
+    """The driver's usage and process-grid checks (src/mpi/gh_higgs_mpi.cpp:35-62) need no GPU."""
+    from gauge_higgs_b200 import mpi_driver
+    assert mpi_driver.main(["gh_higgs_mpi", "fund", "4"]) == 1
+    assert mpi_driver.main(["gh_higgs_mpi", "fund", "6", "1,1,1,4", "2.3", "0.2", "0.5"]) == 1
+    assert mpi_driver.parse(["x", "fund", "8", "2,2", "2.3", "0.2", "0.5"])["P"] == [2, 2, 1, 1]

@@ -25,10 +25,10 @@ def test_halo_pack_order_matches_host_planes():
     V = p.V
     U = (np.arange(V)[:, None, None, None] + 1j * np.arange(36).reshape(1, 4, 3, 3)).astype(np.complex128)
     phi = (np.arange(V)[:, None] * 0.5 + 1j * np.arange(3)[None, :]).astype(np.complex128)
-    h.U = U
-    h.phi = phi
     for field, F, ncomp in ((0, U.reshape(V, 36), 36), (1, phi, 3)):
         for nu in p.split_dirs:
+            h.U = U                   # the unpack below overwrites a plane
+            h.phi = phi
             n = C.c_longlong()
             assert LIB.gh_halo_count(h.ctx.h, 0, field, nu, C.byref(n)) == 0
             sites = p.plane_sites(nu, 1)
@@ -113,3 +113,22 @@ def test_device_metropolis_is_refused_on_a_subdomain():
     with pytest.raises(gh.GaugeHiggsError):
         dom.h[0].trajectory()
     dom.close()
+
+
+def test_mpi_driver_output_does_not_depend_on_the_grid():
+    """gauge_higgs_b200.mpi_driver (src/mpi/gh_higgs_mpi.cpp's command line) in one
+    process: the hot and measured plaquette, L_link, L_phi lines agree for the undivided
+    grid and a 2 x 2 split."""
+    import re
+    import subprocess
+    import sys
+    from conftest import ROOT
+    out = {}
+    for grid in ("1,1,1,1", "1,1,2,2"):
+        r = subprocess.run([sys.executable, "-m", "gauge_higgs_b200.mpi_driver", "fund", "4", grid, "2.3", "0.2", "0.5",
+                            "3", "4", "10", "1.0", "1"], capture_output=True, text=True, cwd=ROOT, timeout=300)
+        assert r.returncode == 0, r.stderr
+        out[grid] = [float(x) for x in re.findall(r"=(-?[0-9]+\.[0-9]+)", "\n".join(
+            ln for ln in r.stdout.splitlines() if ln.startswith(("hot:", "meas:", "acceptance"))))]
+    assert len(out["1,1,1,1"]) == 8
+    assert np.allclose(out["1,1,1,1"], out["1,1,2,2"], rtol=0, atol=2e-10), out
