@@ -528,6 +528,31 @@ def run_extra(a, dist):
                     "launch_floor_ms": round(1e3 / v_floor, 4), "ms_per_ensemble_trajectory": round(1e3 / v, 4),
                     "launch_floor_share": round(v / v_floor, 4), "clocks": clocks})
         ens.close()
+    if wl in ("c5", "all"):
+        from gauge_higgs_b200 import c5 as C5
+        targets = [tuple(float(v) for v in t.split(":")) for t in a.c5_targets.split(",")]
+        sizes = tuple(int(x) for x in a.c5_sizes.split(","))
+        t0 = time.perf_counter()
+        est, cost_s, _ = C5.campaign(targets, sizes=sizes, seed=a.c5_seed)
+        t_camp = time.perf_counter() - t0
+        rows, cost_u = [], 0
+        for (beta, lam) in targets:
+            for L in sizes:
+                ku, cu, _ = C5.uniform_scan(beta, lam, L, seed=a.c5_seed + 500)
+                cost_u += cu
+                kt = C5.truth(beta, lam, L, centre=0.5 * (ku + est[(beta, lam, L)][0]))
+                ks = est[(beta, lam, L)][0]
+                rows.append({"beta": beta, "lambda": lam, "L": L, "kappa_c_truth": round(kt, 4),
+                             "surrogate": round(ks, 4), "surrogate_err": round(ks - kt, 4),
+                             "uniform": round(ku, 4), "uniform_err": round(ku - kt, 4)})
+        out.append({"workload": "C5 learned coupling-scan surrogate (MLP 4-128-128-128-3 x 5 over beta, kappa, lambda, "
+                                "1/L; config-4 batch + space-filling seed data; 32-point active-learning round, "
+                                "1000-trajectory HMC checks)", "targets": rows,
+                    "trajectories_surrogate": cost_s, "trajectories_uniform": cost_u,
+                    "fewer_trajectories": round(cost_u / cost_s, 2),
+                    "within_0.005": {"surrogate": sum(abs(r["surrogate_err"]) <= 0.005 for r in rows),
+                                     "uniform": sum(abs(r["uniform_err"]) <= 0.005 for r in rows), "of": len(rows)},
+                    "campaign_s": round(t_camp, 1)})
     if wl in ("stage0", "all"):
         # the reference's SU(2) -> 2I shakedown point (scripts/su2_stage0.sh: hmc_higgs_multi with
         # rep {12}, d = 13, mu2 = 0.065 and its 13 channel couplings, beta = 2.0, nmd = 20, tau = 1)
@@ -717,7 +742,10 @@ def main():
     ap.add_argument("--validate-traj", type=int, default=2000)
     ap.add_argument("--validate-therm", type=int, default=200)
     ap.add_argument("--c3-ab", action="store_true", help="C3: also time product-path irreps on the tensor path")
-    ap.add_argument("--workload", default="c2", choices=["c2", "c1", "c3", "c4", "big", "stage0", "scan", "validate", "all"],
+    ap.add_argument("--c5-targets", default="2.3:0.5,2.2:0.3", help="C5: beta:lambda targets (comma list)")
+    ap.add_argument("--c5-sizes", default="8,12", help="C5: lattice sizes")
+    ap.add_argument("--c5-seed", type=int, default=100)
+    ap.add_argument("--workload", default="c2", choices=["c2", "c1", "c3", "c4", "c5", "big", "stage0", "scan", "validate", "all"],
                     help="c2 (default) prints the headline line; the others print additional measurements")
     a = ap.parse_args()
     if a.warmup < 3 and a.impl == "ours":
