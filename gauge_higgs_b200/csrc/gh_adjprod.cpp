@@ -231,6 +231,36 @@ bool build(int N, int n, int d, long dimT, const double* Win, Product& out, std:
   out.Q.resize((size_t)A * d);
   const double inv = 1.0 / std::sqrt(best_c2);
   for (size_t i = 0; i < best.size(); ++i) out.Q[i] = best[i] * inv;
+  // the rows the device lifts into: a symmetric / antisymmetric coefficient matrix needs
+  // only the pairs a <= b / a < b
+  out.sym = 0;
+  if (K == 2) {
+    double es = 0.0, ea = 0.0, mx = 0.0;
+    for (int a = 0; a < ng; ++a)
+      for (int b = 0; b < ng; ++b)
+        for (int k = 0; k < d; ++k) {
+          const std::complex<double> x = out.Q[(size_t)(a * ng + b) * d + k], y = out.Q[(size_t)(b * ng + a) * d + k];
+          es = std::max(es, std::abs(x - y));
+          ea = std::max(ea, std::abs(x + y));
+          mx = std::max(mx, std::abs(x));
+        }
+    if (es <= 1e-13 * mx) out.sym = 1;
+    else if (ea <= 1e-13 * mx) out.sym = -1;
+  }
+  out.rows.clear();
+  if (out.sym == 1)
+    for (int a = 0; a < ng; ++a) out.rows.push_back(a * ng + a);
+  out.ndiag = (int)out.rows.size();
+  if (out.sym != 0) {
+    for (int a = 0; a < ng; ++a)
+      for (int b = a + 1; b < ng; ++b) out.rows.push_back(a * ng + b);
+  } else {
+    for (int r = 0; r < A; ++r) out.rows.push_back(r);
+    out.ndiag = A;
+  }
+  out.Qr.resize(out.rows.size() * (size_t)d);
+  for (size_t r = 0; r < out.rows.size(); ++r)
+    for (int k = 0; k < d; ++k) out.Qr[r * d + k] = out.Q[(size_t)out.rows[r] * d + k];
   // against the tensor construction on two generic links
   std::vector<cd> Dp((size_t)d * d), Dt((size_t)d * d);
   for (int which = 0; which < 2; ++which) {

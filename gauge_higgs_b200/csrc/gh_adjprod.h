@@ -29,6 +29,14 @@ struct Product {
   int N = 0, K = 0, d = 0, A = 0;          // A = (N^2 - 1)^K
   std::vector<std::complex<double>> Q;     // [A][d]: isometric intertwiner R -> adjoint^(x)K
   double c2 = 0.0;                         // squared overlap of the chosen slot order
+  // The rows the device lifts into.  K = 2 and every column of Q a symmetric (sym = +1) or
+  // antisymmetric (sym = -1) ng x ng matrix: only the pairs a <= b (a < b) are lifted,
+  // the mirror entry written as +-x, and the projection weights the off-diagonal pairs by 2.
+  // Otherwise (sym = 0) every row.  rows[r] = a ng + b; the first ndiag rows are diagonal.
+  int sym = 0;
+  int ndiag = 0;
+  std::vector<int> rows;
+  std::vector<std::complex<double>> Qr;    // [rows.size()][d]: the rows of Q the device uses
 };
 
 // Builds Q for the irrep whose basis is W ([d][dimT] complex, slot 0 the most

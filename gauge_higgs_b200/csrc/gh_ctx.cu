@@ -454,9 +454,9 @@ int build_general(gh_ctx* ctx, const gh_rep_desc* r) {
   if (!t_v.empty()) CK(cudaMemcpyAsync(v3, t_v.data(), t_v.size() * 16, cudaMemcpyHostToDevice, ctx->st));
   t.wt_ptr = p1; t.wt_l = p2; t.wt_v = v1; t.w_ptr = p3; t.w_i = p4; t.w_v = v2; t.t_ptr = p5; t.t_j = p6; t.t_v = v3;
   t.sp_ptr = nullptr; t.sp_c = nullptr; t.sp_e = nullptr;
-  t.pq64 = nullptr; t.pq32 = nullptr; t.pK = 0;
+  t.pq64 = nullptr; t.pq32 = nullptr; t.prow = nullptr; t.pK = 0; t.pnrows = 0; t.pndiag = 0; t.psym = 0;
   if (ctx->has_prod) {
-    const std::vector<std::complex<double>>& Q = ctx->prod.Q;
+    const std::vector<std::complex<double>>& Q = ctx->prod.Qr;
     std::vector<double2> q64(Q.size());
     std::vector<float2> q32(Q.size());
     for (size_t i = 0; i < Q.size(); ++i) {
@@ -468,8 +468,12 @@ int build_general(gh_ctx* ctx, const gh_rep_desc* r) {
     if ((rc = dalloc(ctx, &d64, q64.size())) || (rc = dalloc(ctx, &d32, q32.size()))) return rc;
     CK(cudaMemcpyAsync(d64, q64.data(), q64.size() * sizeof(double2), cudaMemcpyHostToDevice, ctx->st));
     CK(cudaMemcpyAsync(d32, q32.data(), q32.size() * sizeof(float2), cudaMemcpyHostToDevice, ctx->st));
+    int* rows;
+    if ((rc = dalloc(ctx, &rows, ctx->prod.rows.size()))) return rc;
+    CK(cudaMemcpyAsync(rows, ctx->prod.rows.data(), ctx->prod.rows.size() * sizeof(int), cudaMemcpyHostToDevice, ctx->st));
     CK(cudaStreamSynchronize(ctx->st));     // the host vectors go out of scope
-    t.pq64 = d64; t.pq32 = d32; t.pK = ctx->prod.K;
+    t.pq64 = d64; t.pq32 = d32; t.prow = rows; t.pK = ctx->prod.K;
+    t.pnrows = (int)ctx->prod.rows.size(); t.pndiag = ctx->prod.ndiag; t.psym = ctx->prod.sym;
   }
   t.warp_bytes = (int)ctx->gen_warp_bytes;
   t.px_off = (int)ctx->gen_px_off;

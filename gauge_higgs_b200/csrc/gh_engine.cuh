@@ -84,9 +84,9 @@ struct Engine : EngineBase {
     cudaError_t e = cudaFuncSetAttribute(k_gen_links<D, N, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)gen_smem(b));
     if (e == cudaSuccess && b.gen.pq64) {
       e = b.gen.pK == 1 ? cudaFuncSetAttribute(k_gen_prod<D, N, R, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                               (int)gen_prod_smem<N, 1, C>(b.d))
+                                               (int)gen_prod_smem<N, 1, C>(b.d, b.gen.pnrows))
                         : cudaFuncSetAttribute(k_gen_prod<D, N, R, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                               (int)gen_prod_smem<N, 2, C>(b.d));
+                                               (int)gen_prod_smem<N, 2, C>(b.d, b.gen.pnrows));
     }
     return e == cudaSuccess ? 0 : -1;
   }
@@ -117,8 +117,8 @@ struct Engine : EngineBase {
     a.pot = b.pot; a.sa = b.sa64; a.wpot = b.wpot;
     if (b.gen_prod && b.gen.pq64 && b.pot != POT_MULTI) {   // the potential's w is computed by k_gen_links
       a.work = b.w_gprod;
-      if (b.gen.pK == 1) launch(k_gen_prod<D, N, R, 1>, b.nw_gprod, GP_THREADS, gen_prod_smem<N, 1, C>(b.d), b.st, a);
-      else launch(k_gen_prod<D, N, R, 2>, b.nw_gprod, GP_THREADS, gen_prod_smem<N, 2, C>(b.d), b.st, a);
+      if (b.gen.pK == 1) launch(k_gen_prod<D, N, R, 1>, b.nw_gprod, GP_THREADS, gen_prod_smem<N, 1, C>(b.d, b.gen.pnrows), b.st, a);
+      else launch(k_gen_prod<D, N, R, 2>, b.nw_gprod, GP_THREADS, gen_prod_smem<N, 2, C>(b.d, b.gen.pnrows), b.st, a);
       return;
     }
     const size_t sm = gen_smem(b);

@@ -135,8 +135,11 @@ struct GenTables {                 // general irrep (src/rep/rep_general.hpp), s
   int px_off;                                                // byte offset of px in a warp's region
   // irreps inside the K-fold adjoint product (host: gh_adjprod.h): the isometric
   // intertwiner Q [A][d] in both precisions; null: not available
+  // rows of Q the kernel lifts into (all A, or for a symmetric / antisymmetric coefficient
+  // matrix the pairs a <= b / a < b): prow[r] = a ng + b, the first pndiag diagonal
   const double2* pq64; const float2* pq32;
-  int pK;
+  const int* prow;
+  int pK, pnrows, pndiag, psym;
 };
 
 template <typename R> struct V2;
@@ -834,35 +837,44 @@ template <int N, int K> struct AdjProd {
   static constexpr int A = (K == 1) ? NG : NG * NG;
   static constexpr int RA = (A + 7) / 8;      // rows of A (and of d <= A) per thread
 };
-template <int N, int K, typename C> __host__ __device__ constexpr size_t gen_prod_smem(int d) {
-  return (size_t)(2 * d + AdjProd<N, K>::A) * GP_LINKS * sizeof(cx<C>) +
+template <int N, int K, typename C> __host__ __device__ constexpr size_t gen_prod_smem(int d, int nrows) {
+  return (size_t)nrows * d * sizeof(cx<C>) + (size_t)(2 * d + AdjProd<N, K>::A) * GP_LINKS * sizeof(cx<C>) +
          (size_t)AdjProd<N, K>::NG * AdjProd<N, K>::NG * GP_LINKS * sizeof(C);
 }
 
 // out[i] = (D phi)_k, k = q + 8 i, for the link in lane c; Pin: [d][32] input vectors;
-// X: [A][32] work space; G: [NG][NG][32] adjoint matrices.  Every thread of the block calls it.
+// Qs: [nrows][d] the rows of Q in shared memory; X: [A][32] work space; G: [NG][NG][32]
+// adjoint matrices.  Every thread of the block calls it.
 template <int N, int K, typename C>
-__device__ __forceinline__ void gp_apply(const typename V2<C>::t* __restrict__ Qv, int d, const cx<C>* Pin, cx<C>* X,
+__device__ __forceinline__ void gp_apply(const GenTables& t, const cx<C>* Qs, int d, const cx<C>* Pin, cx<C>* X,
                                          const C* G, bool dag, int c, int q, cx<C>* out) {
   constexpr int NG = AdjProd<N, K>::NG, A = AdjProd<N, K>::A, RA = AdjProd<N, K>::RA, LB = GP_LINKS;
+  const int nr = t.pnrows;
   cx<C> acc[RA];
 #pragma unroll
   for (int i = 0; i < RA; ++i) acc[i] = zero<C>();
-  for (int l = 0; l < d; ++l) {                         // lift: X = Q phi
+  for (int l = 0; l < d; ++l) {                         // lift: the needed rows of X = Q phi
     const cx<C> p = Pin[l * LB + c];
 #pragma unroll
     for (int i = 0; i < RA; ++i) {
       const int r = q + 8 * i;
-      if (r < A) {
-        const typename V2<C>::t v = __ldg(Qv + r * d + l);
-        acc[i] = cfma(acc[i], mk<C>(v.x, v.y), p);
-      }
+      if (r < nr) acc[i] = cfma(acc[i], Qs[r * d + l], p);
     }
   }
   __syncthreads();                                      // earlier readers of X are done
+  if (K == 2 && t.psym < 0 && q < NG) X[(q * NG + q) * LB + c] = zero<C>();   // antisymmetric: zero diagonal
 #pragma unroll
-  for (int i = 0; i < RA; ++i)
-    if (q + 8 * i < A) X[(q + 8 * i) * LB + c] = acc[i];
+  for (int i = 0; i < RA; ++i) {
+    const int r = q + 8 * i;
+    if (r < nr) {
+      const int e = __ldg(t.prow + r);
+      X[e * LB + c] = acc[i];
+      if (K == 2 && t.psym != 0) {
+        const int a = e / NG, b = e - a * NG;
+        if (a != b) X[(b * NG + a) * LB + c] = t.psym > 0 ? acc[i] : mk<C>(-acc[i].re, -acc[i].im);
+      }
+    }
+  }
   __syncthreads();
   auto g = [&](int a, int b) { return dag ? G[(b * NG + a) * LB + c] : G[(a * NG + b) * LB + c]; };
   if constexpr (K == 1) {                               // y = G x
@@ -899,16 +911,17 @@ __device__ __forceinline__ void gp_apply(const typename V2<C>::t* __restrict__ Q
       for (int b = 0; b < NG; ++b) X[(a * NG + b) * LB + c] = y[b];
   }
   __syncthreads();
+  // project: out = Q^dag y over the needed rows; off-diagonal pairs of a symmetric or
+  // antisymmetric coefficient matrix count twice (their mirror entries are equal terms)
 #pragma unroll
-  for (int i = 0; i < RA; ++i) {                        // project: out = Q^dag y
+  for (int i = 0; i < RA; ++i) {
     const int k = q + 8 * i;
-    cx<C> sacc = zero<C>();
-    if (k < d)
-      for (int r = 0; r < A; ++r) {
-        const typename V2<C>::t v = __ldg(Qv + r * d + k);
-        sacc = cfma_cj(sacc, mk<C>(v.x, v.y), X[r * LB + c]);
-      }
-    out[i] = sacc;
+    cx<C> s1 = zero<C>(), s2 = zero<C>();
+    if (k < d) {
+      for (int r = 0; r < t.pndiag; ++r) s1 = cfma_cj(s1, Qs[r * d + k], X[__ldg(t.prow + r) * LB + c]);
+      for (int r = t.pndiag; r < nr; ++r) s2 = cfma_cj(s2, Qs[r * d + k], X[__ldg(t.prow + r) * LB + c]);
+    }
+    out[i] = add(s1, scale(s2, C(2)));
   }
 }
 
@@ -922,12 +935,19 @@ __global__ void __launch_bounds__(GP_THREADS) k_gen_prod(const GenArgs a) {
   const LatDev& L = a.lats[w.lat];
   const int d = a.t.d;
   const int c = threadIdx.x & (LB - 1), q = threadIdx.x >> 5;
-  cx<C>* Px = reinterpret_cast<cx<C>*>(smem_raw);       // [d][32] phi_x
+  cx<C>* Qs = reinterpret_cast<cx<C>*>(smem_raw);       // [nrows][d] the rows of Q the lift uses
+  cx<C>* Px = Qs + a.t.pnrows * d;                      // [d][32] phi_x
   cx<C>* Py = Px + d * LB;                              // [d][32] phi_{x+mu}, then psi_f
   cx<C>* X = Py + d * LB;                               // [A][32]
   C* G = reinterpret_cast<C*>(X + A * LB);              // [NG][NG][32]
-  const typename V2<C>::t* Qv =
-      reinterpret_cast<const typename V2<C>::t*>(sizeof(C) == sizeof(double) ? (const void*)a.t.pq64 : (const void*)a.t.pq32);
+  {
+    const typename V2<C>::t* Qv = reinterpret_cast<const typename V2<C>::t*>(
+        sizeof(C) == sizeof(double) ? (const void*)a.t.pq64 : (const void*)a.t.pq32);
+    for (int i = threadIdx.x; i < a.t.pnrows * d; i += GP_THREADS) {
+      const typename V2<C>::t v = __ldg(Qv + i);
+      Qs[i] = mk<C>(v.x, v.y);
+    }
+  }
   const int mu = w.mu;
   const int s = w.s0 + (c < w.n ? c : 0);              // lanes past the lattice's end compute on site s0
   int x[D];
@@ -957,7 +977,7 @@ __global__ void __launch_bounds__(GP_THREADS) k_gen_prod(const GenArgs a) {
   R* psif = (R*)a.psif;
   R* psib = (R*)a.psib;
   cx<C> o[RA];
-  gp_apply<N, K, C>(Qv, d, Py, X, G, false, c, q, o);  // psi_f = D phi_{x+mu}
+  gp_apply<N, K, C>(a.t, Qs, d, Py, X, G, false, c, q, o);  // psi_f = D phi_{x+mu}
 #pragma unroll
   for (int i = 0; i < RA; ++i) {
     const int k = q + 8 * i;
@@ -967,7 +987,7 @@ __global__ void __launch_bounds__(GP_THREADS) k_gen_prod(const GenArgs a) {
     }
   }
   if (a.mode == 1) return;
-  gp_apply<N, K, C>(Qv, d, Px, X, G, true, c, q, o);   // psi_b = D^dag phi_x
+  gp_apply<N, K, C>(a.t, Qs, d, Px, X, G, true, c, q, o);   // psi_b = D^dag phi_x
 #pragma unroll
   for (int i = 0; i < RA; ++i) {
     const int k = q + 8 * i;
