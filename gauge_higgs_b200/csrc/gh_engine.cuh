@@ -102,12 +102,7 @@ struct Engine : EngineBase {
     const int count = (links ? b.nwk_links : 0) + (do_sites ? b.nwk_sites : 0);
     if (count == 0) return;
     a.work = b.w_kick + first;
-    a.nitems = count;
-#if GH_KICK_CHUNK
-    launch(k_kick<D, N, R, REP>, (unsigned)std::min(count, 148 * KickMinBlocks<R>::v), KICK_BLOCK, 0, b.st, a);
-#else
     launch(k_kick<D, N, R, REP>, count, KICK_BLOCK, 0, b.st, a);
-#endif
   }
   void gen_links(const Bufs& b, double eps, int mode, double* out) override {
     if (REP != REP_GEN) return;

@@ -287,7 +287,6 @@ struct KickArgs {
   double* out;        // M_WRITE destination (SoA like P / like phi, FP64)
   int pot;            // POT_QUARTIC or POT_MULTI
   double mu2;         // multi-invariant potential: -mu2 phi^dag phi
-  int nitems;         // work items of this launch
   PotA sa;            // multi-invariant potential: A = sum_c 2 f_c P_c, values in the field precision
   const double2* wpot;  // general irreps: w = A(M) phi per site, written by k_gen_links
 };
@@ -522,33 +521,15 @@ template <> struct KickMinBlocks<double> {
   static constexpr int v = GH_KICK_MINB_F64 * 128 / KICK_BLOCK > 0 ? GH_KICK_MINB_F64 * 128 / KICK_BLOCK : 1;
 };
 
-#ifndef GH_KICK_CHUNK
-#define GH_KICK_CHUNK 0
-#endif
 template <int D, int N, typename R, int REP>
 __global__ void __launch_bounds__(KICK_BLOCK, KickMinBlocks<R>::v) k_kick(const KickArgs a) {
   pdl_enter();
-#if GH_KICK_CHUNK
-  // each block walks a run of consecutive items (neighbouring tiles of one direction),
-  // so part of a tile's neighbour links are still in this SM's L1 from the previous one
-  const int per = (a.nitems + (int)gridDim.x - 1) / (int)gridDim.x;
-  const int i0 = (int)blockIdx.x * per, i1 = min(i0 + per, a.nitems);
-  for (int it = i0; it < i1; ++it) {
-    const Work w = a.work[it];
-    const LatDev& L = a.lats[w.lat];
-    int s, x[D];
-    if (!tile_site<D>(L, w, threadIdx.x, s, x)) continue;
-    if (w.mu >= 0) kick_link_dispatch<D, N, R, REP>(a, L, w.mu, s, x);
-    else if (REP != REP_NONE) kick_site<D, N, R, REP>(a, L, s, x);
-  }
-#else
   const Work w = a.work[blockIdx.x];
   const LatDev& L = a.lats[w.lat];
   int s, x[D];
   if (!tile_site<D>(L, w, threadIdx.x, s, x)) return;
   if (w.mu >= 0) kick_link_dispatch<D, N, R, REP>(a, L, w.mu, s, x);
   else if (REP != REP_NONE) kick_site<D, N, R, REP>(a, L, s, x);
-#endif
 }
 
 // ---------------------------------------------------------------------------
