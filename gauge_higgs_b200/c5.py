@@ -11,8 +11,11 @@ active-learning round places 32 new coupling points where the members disagree m
 about the transition (the spread of d<L_link>/dkappa, which is 2 D chi_link: its
 maximum is the chi_link peak, the reference's transition locator,
 validate_su2higgs.sh), near each target's predicted peak, and checks every point by
-plain HMC (1000 trajectories at 8^4 and 12^4).  kappa_c of a target (beta, lambda, L)
-is the maximum of the predicted slope, median over members.
+plain HMC (1000 trajectories at 8^4 and 12^4).  Those checks are the judge: kappa_c of
+a target (beta, lambda, L) is the maximum of a concave quadratic fitted to log chi_link at
+its checked points (the surrogate steered them to bracket the peak); the surrogate's own
+estimate, the maximum of its predicted slope (median over members), is kept beside it
+and is the fallback where the checks do not bracket a peak.
 
 The method without the surrogate is a uniform batched scan of kappa over the domain at
 the asked resolution (0.005) with the same per-point statistics, one per target and
@@ -47,7 +50,7 @@ def run_points(points, ntherm, nmeas, nmd=12, precision="fp32", seed0=1):
     ll = rec["L_link"]
     out = {"beta": pts[:, 0], "kappa": pts[:, 1], "lam": pts[:, 2], "L": L, "L_link": ll.mean(0),
            "chi": (L.astype(float) ** D) * ll.var(0), "plaq": rec["plaquette"].mean(0),
-           "acc": rec["accepted"].mean(0)}
+           "acc": rec["accepted"].mean(0), "nmeas": np.full(n, nmeas)}
     return out, n * (ntherm + nmeas)
 
 
@@ -132,10 +135,27 @@ def choose(sur, targets, sizes, per_round, window=0.03, spacing=0.003, h=5e-4):
     return out
 
 
+def hmc_peak(data, beta, lam, L, min_meas):
+    """kappa_c judged by plain HMC: the maximum of a quadratic in kappa fitted to log chi_link
+    at the checked points of (beta, lambda, L) (those with at least min_meas measured
+    trajectories), inside their span; None when the fit is not concave there."""
+    sel = (np.isclose(data["beta"], beta) & np.isclose(data["lam"], lam) & (data["L"] == L) &
+           (data["nmeas"] >= min_meas))
+    k, y = data["kappa"][sel], np.log(np.maximum(data["chi"][sel], 1e-12))
+    if len(k) < 4:
+        return None
+    a, b, _ = np.polyfit(k - k.mean(), y, 2)
+    if not a < 0:
+        return None
+    kc = k.mean() - b / (2 * a)
+    return float(kc) if k.min() <= kc <= k.max() else None
+
+
 def campaign(targets, sizes=(8, 12), rounds=1, per_round=32, n_space=32, seed=100, seed_therm=50, seed_meas=150,
              check_therm=100, check_meas=1000, precision="fp32"):
-    """The surrogate-steered search.  Returns ({(beta, lambda, L): (kappa_c, spread)},
-    trajectories spent, the data)."""
+    """The surrogate-steered search.  Returns ({(beta, lambda, L): (kappa_c, surrogate's
+    kappa_c, surrogate's spread)}, trajectories spent, the data).  kappa_c is judged by the
+    HMC checks (hmc_peak) where they bracket a peak, else the surrogate's estimate."""
     rng = np.random.default_rng(seed)
     data, cost = run_points(c4_points() + space_filling(n_space, sizes, rng), seed_therm, seed_meas,
                             precision=precision, seed0=seed)
@@ -147,7 +167,12 @@ def campaign(targets, sizes=(8, 12), rounds=1, per_round=32, n_space=32, seed=10
         data = merge(data, new)
         cost += c
         sur.fit(data, seed=7 + r)
-    est = {(b, lam, L): sur.kappa_c(b, lam, L) for (b, lam) in targets for L in sizes}
+    est = {}
+    for (b, lam) in targets:
+        for L in sizes:
+            ks, sd = sur.kappa_c(b, lam, L)
+            kh = hmc_peak(data, b, lam, L, check_meas)
+            est[(b, lam, L)] = (kh if kh is not None else ks, ks, sd)
     sur.close()
     return est, cost, data
 
