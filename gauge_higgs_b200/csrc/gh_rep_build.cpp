@@ -15,6 +15,8 @@
 #include <cmath>
 #include <complex>
 #include <numeric>
+#include <map>
+#include <functional>
 #include <vector>
 #include "../../include/gauge_higgs_b200.h"
 
@@ -83,21 +85,23 @@ struct Builder {
     signs.resize(perms.size());
     for (size_t i = 0; i < perms.size(); ++i) signs[i] = parity_sign(perms[i]);
   }
+  // Single-row diagram {n}: one basis vector per multiset of n slot indices, the
+  // normalised sum of every tensor index whose digits form that multiset.  The order is
+  // the reference's (ascending sorted tuples), which is the digit histograms in
+  // descending lexicographic order: at the first value where two histograms differ, the
+  // one with more copies of it has that value where the other's tuple has a larger one.
   void basis_symmetric() {
-    std::vector<int> t(n, 0);
-    while (true) {
+    std::map<std::vector<int>, std::vector<long>, std::greater<std::vector<int>>> by_hist;
+    for (long t = 0; t < dimT; ++t) {
+      std::vector<int> hist(N, 0);
+      for (int digit : idx2tup(t)) ++hist[digit];
+      by_hist[hist].push_back(t);
+    }
+    for (const auto& group : by_hist) {
       std::vector<cd> v(dimT, cd(0, 0));
-      std::vector<int> perm = t;
-      long count = 0;
-      do { v[tup2idx(perm)] = cd(1, 0); ++count; } while (std::next_permutation(perm.begin(), perm.end()));
-      const double inv = 1.0 / std::sqrt((double)count);
-      for (auto& z : v) z *= cd(inv, 0);
+      const double w = 1.0 / std::sqrt((double)group.second.size());
+      for (long t : group.second) v[t] = cd(w, 0);
       W.push_back(v);
-      int j = n - 1;
-      while (j >= 0 && t[j] == N - 1) --j;
-      if (j < 0) break;
-      ++t[j];
-      for (int k = j + 1; k < n; ++k) t[k] = t[j];
     }
   }
   void basis_young() {
