@@ -1063,11 +1063,8 @@ struct DriftArgs {
   int d;
   int frozen;          // |phi_x| = 1: geodesic (great-circle) drift of (phi, pi)
 };
-#ifndef GH_DRIFT_MINB
-#define GH_DRIFT_MINB 1
-#endif
 template <int N, typename R, typename A>
-__global__ void __launch_bounds__(KBLOCK, GH_DRIFT_MINB) k_drift(const DriftArgs a) {
+__global__ void __launch_bounds__(KBLOCK) k_drift(const DriftArgs a) {
   pdl_enter();
   const Work w = a.work[blockIdx.x];
   if ((int)threadIdx.x >= w.n) return;
