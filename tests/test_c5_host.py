@@ -54,15 +54,8 @@ def test_c4_points_are_configuration_4():
     assert np.all(pts[:, 0] == 2.3) and np.all(pts[:, 2] == 0.5)
 
 
-def test_hmc_peak_fits_the_checked_points_only():
-    k = np.linspace(0.24, 0.26, 8)
-    chi = np.exp(2.0 - ((k - 0.2512) / 0.01) ** 2)
-    data = {"beta": np.full(8, 2.2), "lam": np.full(8, 0.3), "L": np.full(8, 8), "kappa": k, "chi": chi,
-            "nmeas": np.full(8, 1000)}
-    # a short-run point far off must not enter the fit
-    extra = {"beta": [2.2], "lam": [0.3], "L": [8], "kappa": [0.30], "chi": [50.0], "nmeas": [150]}
-    data = {key: np.concatenate([data[key], np.asarray(extra[key], float if key != "L" else int)]) for key in data}
-    assert abs(c5.hmc_peak(data, 2.2, 0.3, 8, 1000) - 0.2512) < 1e-6
-    # no concave peak inside the checked span: no verdict (the surrogate's estimate stands)
-    data["chi"][:8] = np.exp(k * 40)
-    assert c5.hmc_peak(data, 2.2, 0.3, 8, 1000) is None
+def test_weighted_repeats_only_the_checked_points():
+    data = {"kappa": np.array([0.2, 0.25, 0.3]), "nmeas": np.array([150, 1000, 150]), "L": np.array([8, 8, 12])}
+    w = c5.weighted(data, 1000, 4)
+    assert len(w["kappa"]) == 6
+    assert np.sum(w["kappa"] == 0.25) == 4 and np.sum(w["kappa"] == 0.2) == 1

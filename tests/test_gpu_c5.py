@@ -8,8 +8,8 @@ the predicted chi_link peaks, each checked by 1000-trajectory plain HMC at 8^4 a
 Without the surrogate: one uniform batched scan per target and size, kappa over the
 domain [0.15, 0.35] at the asked resolution (0.005) with the same per-point statistics,
 and its chi_link peak.  Truth: a dense high-statistics chi_link peak (not counted).
-kappa_c of the campaign is judged by its 1000-trajectory HMC checks (a concave fit of log
-chi_link over the points the surrogate placed around the peak).  The test asks for kappa_c
+kappa_c of the campaign is the network's after a last fit in which each 1000-trajectory
+HMC check counts four times.  The test asks for kappa_c
 to +-0.005 on every target with at least 3x fewer HMC trajectories than the uniform scans.  Every point of every method is plain HMC on the
 GPU; the computation is deterministic for fixed seeds."""
 import numpy as np
@@ -33,8 +33,8 @@ def test_surrogate_campaign_locates_kappa_c_with_fewer_trajectories():
             ks, ka, _ = est[(beta, lam, L)]
             kt = c5.truth(beta, lam, L, centre=0.5 * (ks + ku))
             rows.append((beta, lam, L, kt, ks, ku))
-            print(f"\nbeta {beta} lambda {lam} L {L}: truth {kt:.4f}  surrogate-steered {ks:.4f} ({ks - kt:+.4f}; "
-                  f"network alone {ka:.4f})  uniform {ku:.4f} ({ku - kt:+.4f})")
+            print(f"\nbeta {beta} lambda {lam} L {L}: truth {kt:.4f}  surrogate {ks:.4f} ({ks - kt:+.4f}; "
+                  f"checks unweighted {ka:.4f})  uniform {ku:.4f} ({ku - kt:+.4f})")
     print(f"trajectories: surrogate {cost_s}, uniform scans {cost_u} ({cost_u / cost_s:.2f}x)")
     err_s = np.array([abs(r[4] - r[3]) for r in rows])
     assert cost_u >= 3 * cost_s
