@@ -89,16 +89,43 @@ class Dist:
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled during a timed region."""
+    """SM clock and throttle reasons sampled during a timed region: NVML polled from a
+    background thread every 2 ms (a timed region of a few tens of ms still gets samples),
+    or nvidia-smi at its 100 ms minimum when NVML is not available."""
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
          "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
          "clocks_event_reasons.sw_power_cap")
+    NAMES = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
 
     def __init__(self, gpu_index):
         self.idx = gpu_index
         self.p = None
+        self.thread = None
 
     def start(self):
+        try:
+            import threading
+            import pynvml as nv
+            nv.nvmlInit()
+            h = nv.nvmlDeviceGetHandleByIndex(self.idx)
+            self.mx = nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM)
+            bits = {"hw_slowdown": nv.nvmlClocksEventReasonHwSlowdown,
+                    "hw_thermal_slowdown": nv.nvmlClocksEventReasonHwThermalSlowdown,
+                    "sw_thermal_slowdown": nv.nvmlClocksEventReasonSwThermalSlowdown,
+                    "sw_power_cap": nv.nvmlClocksEventReasonSwPowerCap}
+            self.sm, self.reasons, self.stop_ev = [], set(), threading.Event()
+
+            def poll():
+                while not self.stop_ev.is_set():
+                    self.sm.append(nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM))
+                    r = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
+                    self.reasons.update(n for n, b in bits.items() if r & b)
+                    self.stop_ev.wait(0.002)
+            self.thread = threading.Thread(target=poll, daemon=True)
+            self.thread.start()
+            return
+        except Exception:
+            self.thread = None
         self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
         try:
             self.p = subprocess.Popen(["nvidia-smi", "-i", str(self.idx), f"--query-gpu={self.Q}",
@@ -108,6 +135,13 @@ class ClockSampler:
             self.p = None
 
     def stop(self):
+        if self.thread is not None:
+            self.stop_ev.set()
+            self.thread.join(timeout=5)
+            if not self.sm:
+                return None
+            return {"sm_mhz": statistics.median(self.sm), "sm_max_mhz": float(self.mx), "reasons": sorted(self.reasons),
+                    "samples": len(self.sm), "source": "nvml"}
         if self.p is None:
             return None
         self.p.terminate()
@@ -119,7 +153,6 @@ class ClockSampler:
         rows = [r.split(",") for r in open(self.f.name).read().strip().splitlines() if r.strip()]
         os.unlink(self.f.name)
         sm, mx, reasons = [], None, set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         for r in rows:
             r = [x.strip() for x in r]
             if len(r) < 9:
@@ -129,12 +162,13 @@ class ClockSampler:
                 mx = float(r[2])
             except ValueError:
                 continue
-            for n, v in zip(names, r[5:9]):
+            for n, v in zip(self.NAMES, r[5:9]):
                 if v.lower() == "active":
                     reasons.add(n)
         if not sm:
             return None
-        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm),
+                "source": "nvidia-smi"}
 
 
 def launches_per_traj(nmd, prec):
