@@ -770,7 +770,7 @@ def main():
     ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--cpu-traj", type=int, default=3)
+    ap.add_argument("--cpu-traj", type=int, default=10)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--stage0-sizes", default="4,8", help="lattice extents of --workload stage0 (comma list)")
     ap.add_argument("--c3-reps", default="sextet,octet,27plet", help="irreps of --workload c3 (comma list)")

@@ -122,11 +122,15 @@ struct Engine : EngineBase {
   void drift(const Bufs& b, double eps, int reunit) override {
     DriftArgs a;
     a.work = b.w_all; a.lats = b.lats; a.U = b.U; a.P = b.P; a.phi = b.phi; a.pi = b.pi;
-    a.eps = eps; a.reunit = reunit != 0; a.d = b.d; a.frozen = b.frozen;
+    a.eps = eps; a.d = b.d; a.frozen = b.frozen;
     const unsigned nb = b.nw_links + (b.scalar ? b.nw_sites : 0);
-    // reunit 2: the all-FP32 link update (GH_PREC_FP32_ALL); otherwise FP64 arithmetic
-    if (sizeof(R) != sizeof(double) && reunit == 2) launch(k_drift<N, R, float>, nb, KBLOCK, 0, b.st, a);
-    else launch(k_drift<N, R, double>, nb, KBLOCK, 0, b.st, a);
+    // reunit 2: the all-FP32 link update (GH_PREC_FP32_ALL); otherwise FP64 arithmetic,
+    // projected back to SU(N) (1) or not (0, the FP64 mode)
+    if constexpr (sizeof(R) != sizeof(double)) {
+      if (reunit == 2) { launch(k_drift<N, R, float, true>, nb, KBLOCK, 0, b.st, a); return; }
+    }
+    if (reunit) launch(k_drift<N, R, double, true>, nb, KBLOCK, 0, b.st, a);
+    else launch(k_drift<N, R, double, false>, nb, KBLOCK, 0, b.st, a);
   }
   void sphere(const Bufs& b, int what) override {
     if (!b.scalar) return;

@@ -315,8 +315,11 @@ __device__ __forceinline__ void kick_link(const KickArgs& a, const LatDev& L, in
       const int smn = nbwd(L, s, x[nu], nu);
       const int spm_mn = nbwd(L, spm, x[nu], nu);
       // upper staple U_nu(x+mu) U_mu(x+nu)^dag U_nu(x)^dag, lower U_nu(x+mu-nu)^dag U_mu(x-nu)^dag U_nu(x-nu)
-      mm_nd_acc(sig, mm_nd(ld_link<N, C>(U, L, nu, spm), ld_link<N, C>(U, L, mu, spn)), ld_link<N, C>(U, L, nu, s));
-      mm_acc(sig, mm_dd(ld_link<N, C>(U, L, nu, spm_mn), ld_link<N, C>(U, L, mu, smn)), ld_link<N, C>(U, L, nu, smn));
+      // (the inner products of two links through mm_su: their last row from unitarity)
+      mm_nd_acc(sig, mm_su<N, C, false, true>(ld_link<N, C>(U, L, nu, spm), ld_link<N, C>(U, L, mu, spn)),
+                ld_link<N, C>(U, L, nu, s));
+      mm_acc(sig, mm_su<N, C, true, true>(ld_link<N, C>(U, L, nu, spm_mn), ld_link<N, C>(U, L, mu, smn)),
+             ld_link<N, C>(U, L, nu, smn));
     }
     Umu = ld_link<N, C>(U, L, mu, s);
     Om = mm(Umu, sig);
@@ -1059,11 +1062,11 @@ struct DriftArgs {
   void* phi;
   void* pi;
   double eps;
-  int reunit;
   int d;
   int frozen;          // |phi_x| = 1: geodesic (great-circle) drift of (phi, pi)
 };
-template <int N, typename R, typename A>
+// PROJ: the link update is projected back to SU(N) (the FP32 modes' drift)
+template <int N, typename R, typename A, bool PROJ>
 __global__ void __launch_bounds__(KBLOCK) k_drift(const DriftArgs a) {
   pdl_enter();
   const Work w = a.work[blockIdx.x];
@@ -1083,8 +1086,16 @@ __global__ void __launch_bounds__(KBLOCK) k_drift(const DriftArgs a) {
 #pragma unroll
     for (int i = 0; i < N * N; ++i) H.e[i] = scale(H.e[i], (A)a.eps);
     const Mat<N, A> E = expi<N>(H);
-    Mat<N, A> Un = mm(E, ld_link_rw<N, A>((const R*)a.U, L, mu, s));
-    if (a.reunit) project_su<N, A>(Un);
+    const Mat<N, A> Uo = ld_link_rw<N, A>((const R*)a.U, L, mu, s);
+    Mat<N, A> Un;
+    if constexpr (PROJ) {
+      // the projection reads the first N-1 rows of E U and rebuilds the last, so the
+      // last row of the product (and of E) is never formed
+      mm_core<N, A, false, false, false, N - 1>(E, Uo, Un);
+      project_su<N, A>(Un);
+    } else {
+      Un = mm(E, Uo);
+    }
     st_link<N, A>((R*)a.U, L, mu, s, Un);
   } else if (a.frozen) {
     // Frozen length (src/hmc/gauge_higgs_hmc.hpp:84-102): the exact constrained free

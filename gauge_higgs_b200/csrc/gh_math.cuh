@@ -92,10 +92,11 @@ template <typename T> GH_HD cx<T> cfma_cj(cx<T> s, cx<T> a, cx<T> b) {
 // multiply-accumulate is 4 FMAs (re += ar br -/+ ai bi, im += ar bi +/- ai br, the
 // conjugation signs folded into operand negations), where the written-out form
 // s + (ar br - ai bi) costs 6 (one product of each pair cannot fuse).
-template <int N, typename T, bool DA, bool DB, bool ACC>
+// Rows 0 .. ROWS-1 of the output only.
+template <int N, typename T, bool DA, bool DB, bool ACC, int ROWS = N>
 GH_HD void mm_core(const Mat<N, T>& A, const Mat<N, T>& B, Mat<N, T>& C) {
 #pragma unroll
-  for (int i = 0; i < N; ++i)
+  for (int i = 0; i < ROWS; ++i)
 #pragma unroll
     for (int j = 0; j < N; ++j) {
       cx<T> s = ACC ? C.e[i * N + j] : zero<T>();
@@ -137,6 +138,41 @@ template <int N, typename T> GH_HD Mat<N, T> mm_dn(const Mat<N, T>& A, const Mat
 template <int N, typename T> GH_HD Mat<N, T> mm_dd(const Mat<N, T>& A, const Mat<N, T>& B) {
   Mat<N, T> C;
   mm_core<N, T, true, true, false>(A, B, C);
+  return C;
+}
+// conj(a b - c d), one chain of fused multiply-adds per part
+template <typename T> GH_HD cx<T> conj_cross(const cx<T>& a, const cx<T>& b, const cx<T>& c, const cx<T>& d) {
+  T re = c.im * d.im;
+  re = fmad(-c.re, d.re, re);
+  re = fmad(-a.im, b.im, re);
+  re = fmad(a.re, b.re, re);
+  T im = c.re * d.im;
+  im = fmad(c.im, d.re, im);
+  im = fmad(-a.re, b.im, im);
+  im = fmad(-a.im, b.re, im);
+  return mk<T>(re, im);
+}
+// Product of two SU(N) matrices, N = 2 or 3: the first N-1 rows as products, the last
+// from them through unitarity and det = 1 (SU(3): row 2 = conj(row 0 x row 1); SU(2):
+// row 1 = (-conj c01, conj c00)).  The last row costs 24 multiply-adds instead of 36
+// (SU(3)), and the operand entries only it would read -- the last row of op(A) -- are
+// never used, so their loads drop out.  The result differs from the full product by
+// the operands' distance from SU(N) (rounding level for links of the HMC state).
+// Other N: the full product.
+template <int N, typename T, bool DA, bool DB> GH_HD Mat<N, T> mm_su(const Mat<N, T>& A, const Mat<N, T>& B) {
+  Mat<N, T> C;
+  if constexpr (N == 3) {
+    mm_core<N, T, DA, DB, false, 2>(A, B, C);
+    C.e[6] = conj_cross(C.e[1], C.e[5], C.e[2], C.e[4]);
+    C.e[7] = conj_cross(C.e[2], C.e[3], C.e[0], C.e[5]);
+    C.e[8] = conj_cross(C.e[0], C.e[4], C.e[1], C.e[3]);
+  } else if constexpr (N == 2) {
+    mm_core<N, T, DA, DB, false, 1>(A, B, C);
+    C.e[2] = mk<T>(-C.e[1].re, C.e[1].im);
+    C.e[3] = mk<T>(C.e[0].re, -C.e[0].im);
+  } else {
+    mm_core<N, T, DA, DB, false>(A, B, C);
+  }
   return C;
 }
 // C += A B ; C += A B^dag
@@ -281,7 +317,7 @@ template <int N, typename T> GH_HD Mat<N, T> expi_series(const Mat<N, T>& H) {
   const T nrm = sqrt(fnorm2(H));
   int s = 0;
   T scaled = nrm;
-  while (scaled > T(0.5)) { scaled *= T(0.5); ++s; }
+  while (scaled > T(0.5) && s < 64) { scaled *= T(0.5); ++s; }   // bounded: a non-finite H ends as NaN
   const T inv2s = (T)ldexp(1.0, -s);
   Mat<N, T> A, term, res;
 #pragma unroll
@@ -339,7 +375,7 @@ template <typename T> GH_HD Mat<3, T> herm_sq3(const Mat<3, T>& Q) {
 template <typename T> GH_HD Mat<3, T> expi3(const Mat<3, T>& H) {
   T nrm2 = fnorm2(H);               // scale until ||H||_F / 2^s <= 1/2, compared squared
   int s = 0;
-  while (nrm2 > T(0.25)) { nrm2 *= T(0.25); ++s; }
+  while (nrm2 > T(0.25) && s < 64) { nrm2 *= T(0.25); ++s; }   // bounded: a non-finite H ends as NaN
   const T sc = (T)ldexp(1.0, -s);
   Mat<3, T> Q;
 #pragma unroll
