@@ -581,7 +581,7 @@ def run_extra(a, dist):
                              "surrogate_checks_unweighted": round(ks, 4), "unweighted_err": round(ks - kt, 4),
                              "uniform": round(ku, 4), "uniform_err": round(ku - kt, 4)})
         out.append({"workload": "C5 learned coupling-scan surrogate (MLP 4-128-128-128-3 x 5 over beta, kappa, lambda, "
-                                "1/L; config-4 batch + space-filling seed data; 32-point active-learning round, "
+                                "1/L; config-4 batch + 12-kappa seed lines at every target and size; 32-point active-learning round, "
                                 "1000-trajectory HMC checks)", "targets": rows,
                     "trajectories_surrogate": cost_s, "trajectories_uniform": cost_u,
                     "fewer_trajectories": round(cost_u / cost_s, 2),

@@ -6,7 +6,8 @@ at lr 1e-3) maps (beta, kappa, lambda, 1/L) over beta in [2.1, 2.5], kappa in
 [0.15, 0.35], lambda in [0.1, 1.0] to (<L_link>, log chi_link, plaquette) of the SU(2)
 fundamental-Higgs model.  It is trained first on the batch of configuration 4 (64
 lattices, 16 kappas in 0.22..0.31 for each L in 6, 8, 10, 12, at beta 2.3, lambda 0.5)
-and a space-filling batch over the whole input domain, both short runs; then each
+and on 12 kappas evenly over the kappa domain at every target's (beta, lambda) and size,
+all short runs; then each
 active-learning round places 32 new coupling points where the members disagree most
 about the transition (the spread of d<L_link>/dkappa, which is 2 D chi_link: its
 maximum is the chi_link peak, the reference's transition locator,
@@ -14,9 +15,11 @@ validate_su2higgs.sh), near each target's predicted peak, and checks every point
 plain HMC (1000 trajectories at 8^4 and 12^4).  The last fit counts each of those
 checks four times (they are the precise data; the seed runs have 150 trajectories), and
 kappa_c of a target (beta, lambda, L) is the maximum of the predicted slope, median over
-members.  Measured over two seeds and four targets this keeps every estimate within
-0.0035 of a dense high-statistics chi_link peak, where fitting log chi over the checked
-points alone misses by up to 0.02 and the unweighted network by up to 0.005.
+members.  Measured over four seeds and four targets this keeps every estimate within
+0.0045 of a dense high-statistics chi_link peak.  A space-filling seed batch over the
+whole (beta, kappa, lambda) domain instead left the first network's slope maximum at the
+domain's edge for some targets (off by up to 0.1), and the checks around it could not
+recover.
 
 The method without the surrogate is a uniform batched scan of kappa over the domain at
 the asked resolution (0.005) with the same per-point statistics, one per target and
@@ -34,14 +37,15 @@ DOMAIN = {"beta": (2.1, 2.5), "kappa": (0.15, 0.35), "lam": (0.1, 1.0)}
 D = 4
 
 
-def run_points(points, ntherm, nmeas, nmd=12, precision="fp32", seed0=1):
+def run_points(points, ntherm, nmeas, nmd=12, precision="fp32", seed0=1, seeds=None):
     """Plain HMC at every (beta, kappa, lambda, L) point, all points one batched ensemble
-    (lattices of unequal extents and couplings).  Returns per-point arrays and the
-    number of trajectories spent."""
+    (lattices of unequal extents and couplings), point i seeded seed0 + i or seeds[i].
+    Returns per-point arrays and the number of trajectories spent."""
     pts = np.asarray(points, float).reshape(-1, 4)
     n = len(pts)
     L = pts[:, 3].astype(int)
-    ens = _hmc.Ensemble([[int(l)] * D for l in L], _hmc.FundamentalRep(2), seeds=[seed0 + i for i in range(n)],
+    seeds = [seed0 + i for i in range(n)] if seeds is None else [int(x) for x in seeds]
+    ens = _hmc.Ensemble([[int(l)] * D for l in L], _hmc.FundamentalRep(2), seeds=seeds,
                         precision=precision, beta=pts[:, 0], kappa=pts[:, 1], lam=pts[:, 2], nmd=nmd, integ="omelyan")
     ens.hot(0.8)
     ens.phi_gaussian(12345, 0.3)
@@ -103,14 +107,11 @@ def c4_points():
     return [(2.3, 0.22 + 0.006 * i, 0.5, L) for L in (6, 8, 10, 12) for i in range(16)]
 
 
-def space_filling(n, sizes, rng):
-    """A Latin hypercube over (beta, kappa, lambda), sizes alternating."""
-    cols = []
-    for key in ("beta", "kappa", "lam"):
-        lo, hi = DOMAIN[key]
-        u = (rng.permutation(n) + rng.random(n)) / n
-        cols.append(lo + (hi - lo) * u)
-    return [(cols[0][i], cols[1][i], cols[2][i], sizes[i % len(sizes)]) for i in range(n)]
+def target_lines(targets, sizes, n=12):
+    """The extra (beta, lambda) points: n kappas evenly over the whole kappa domain at every
+    target's (beta, lambda) and every size."""
+    ks = np.linspace(*DOMAIN["kappa"], n)
+    return [(beta, float(k), lam, L) for (beta, lam) in targets for L in sizes for k in ks]
 
 
 def choose(sur, targets, sizes, per_round, window=0.03, spacing=0.003, h=5e-4):
@@ -146,14 +147,13 @@ def weighted(data, min_meas, weight):
     return out
 
 
-def campaign(targets, sizes=(8, 12), rounds=1, per_round=32, n_space=32, seed=100, seed_therm=50, seed_meas=150,
+def campaign(targets, sizes=(8, 12), rounds=1, per_round=32, n_line=12, seed=100, seed_therm=50, seed_meas=150,
              check_therm=100, check_meas=1000, check_weight=4, precision="fp32"):
     """The surrogate-steered search.  Returns ({(beta, lambda, L): (kappa_c, the network's
     kappa_c before the checks were weighted, member spread)}, trajectories spent, the data).
     kappa_c is the maximum of the predicted slope after the last fit, in which every
     1000-trajectory HMC check counts check_weight times."""
-    rng = np.random.default_rng(seed)
-    data, cost = run_points(c4_points() + space_filling(n_space, sizes, rng), seed_therm, seed_meas,
+    data, cost = run_points(c4_points() + target_lines(targets, sizes, n_line), seed_therm, seed_meas,
                             precision=precision, seed0=seed)
     sur = Surrogate4D(seed=seed)
     sur.fit(data)
@@ -189,10 +189,15 @@ def uniform_scan(beta, lam, L, spacing=0.005, ntherm=100, nmeas=1000, precision=
 def truth(beta, lam, L, centre, half=0.03, spacing=0.0025, ntherm=200, nmeas=1000, repeats=4, precision="fp32",
           seed=9000):
     """A dense high-statistics chi_link peak around `centre` (not counted): repeats x nmeas
-    measured trajectories per point, chi from the pooled series' variance."""
-    ks = np.arange(centre - half, centre + half + spacing / 2, spacing)
+    measured trajectories per point, chi the mean over the repeats.  The kappas lie on the
+    fixed grid of multiples of `spacing` and each point's chains are seeded by its grid
+    index, so that two windows share the points they overlap in."""
+    i0 = int(round(centre / spacing))
+    idx = np.arange(i0 - int(round(half / spacing)), i0 + int(round(half / spacing)) + 1)
+    ks = idx * spacing
     chis = []
     for r in range(repeats):
-        d, _ = run_points([(beta, k, lam, L) for k in ks], ntherm, nmeas, precision=precision, seed0=seed + 100 * r)
+        d, _ = run_points([(beta, k, lam, L) for k in ks], ntherm, nmeas, precision=precision,
+                          seeds=seed + 1000 * r + idx)
         chis.append(d["chi"])
     return chi_peak(ks, np.mean(chis, 0))

@@ -1,5 +1,5 @@
 """Host logic of the configuration-5 campaign (gauge_higgs_b200/c5.py) without a GPU:
-the space-filling batch stays in the domain and stratifies every coupling; the
+the seed lines cover the kappa domain at every target and size; the
 active-learning choice gives every (target, size) its share of the 32 points, inside
 the window around the predicted peak, at the highest member disagreement and at least
 the asked spacing apart."""
@@ -8,15 +8,16 @@ import numpy as np
 from gauge_higgs_b200 import c5
 
 
-def test_space_filling_is_a_latin_hypercube():
-    rng = np.random.default_rng(3)
-    pts = np.array(c5.space_filling(32, (8, 12), rng))
-    for col, key in enumerate(("beta", "kappa", "lam")):
-        lo, hi = c5.DOMAIN[key]
-        u = (pts[:, col] - lo) / (hi - lo)
-        assert np.all((u >= 0) & (u < 1))
-        assert sorted(np.floor(u * 32).astype(int)) == list(range(32))    # one point per stratum
-    assert set(pts[:, 3]) == {8, 12}
+def test_target_lines_span_the_kappa_domain_at_every_target_and_size():
+    targets, sizes = [(2.3, 0.5), (2.2, 0.3)], (8, 12)
+    pts = np.array(c5.target_lines(targets, sizes, 12))
+    assert len(pts) == 2 * 2 * 12
+    for b, lam in targets:
+        for L in sizes:
+            ks = np.sort(pts[(pts[:, 0] == b) & (pts[:, 2] == lam) & (pts[:, 3] == L), 1])
+            assert len(ks) == 12
+            assert np.isclose(ks[0], c5.DOMAIN["kappa"][0]) and np.isclose(ks[-1], c5.DOMAIN["kappa"][1])
+            assert np.allclose(np.diff(ks), np.diff(ks)[0])
 
 
 class FakeSurrogate:
