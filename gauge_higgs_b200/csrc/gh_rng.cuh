@@ -199,12 +199,84 @@ GH_HD double cr_cos(double x) {
   return add_rn(res.hi, res.lo);
 }
 
+// Two-phase evaluation (Ziv's strategy): a first phase accurate to ~2^-66 whose
+// result comes with an error bound E; when hi + lo - E and hi + lo + E round to the
+// same double, that double is the correctly rounded value, and the first phase
+// returns it.  Otherwise (about one call in 2^12) the double-double evaluation
+// above decides.  Either way the result is the one cr_log / cr_cos give.
+GH_HD bool ziv_round(dd r, double E, double* y) {
+  const double a = add_rn(r.hi, add_rn(r.lo, E)), b = add_rn(r.hi, sub_rn(r.lo, E));
+  *y = add_rn(r.hi, r.lo);
+  return a == b;
+}
+
+// log x, first phase: the reduction of cr_log, then log m = log c + 2s + tail with the
+// tail 2s (s^2/3 + s^4/5 + s^6/7 + s^8/9) in double (it is below 2^-18 of 2s for
+// |s| < 0.0028; the terms dropped are below 2^-86 of 2s).  Error: the tail's rounding,
+// under 2^-70 |2s|, and the double-double steps, under 2^-100 |log x|; E doubles both.
+GH_HD double cr_log_fast(double x) {
+  const uint64_t bits = dbits(x);
+  int e = (int)((bits >> 52) & 0x7FF) - 1023;
+  double m = bitsd((bits & 0x000FFFFFFFFFFFFFULL) | 0x3FF0000000000000ULL);
+  if (m > 1.4142135623730951) { m = mul_rn(m, 0.5); e += 1; }
+  const double ci = rint_rn(mul_rn(m, 128.0));
+  const int i = (int)ci;
+  const double c = mul_rn(ci, 0.0078125);
+  const double t = sub_rn(m, c);
+  const dd s = dd_div(dd{t, 0.0}, two_sum(mul_rn(2.0, c), t));
+  const double z = mul_rn(s.hi, s.hi);
+  double q = fma_rn(z, 0.1111111111111111, 0.14285714285714285);    // 1/9, 1/7
+  q = fma_rn(z, q, 0.2);
+  q = fma_rn(z, q, 0.3333333333333333);
+  const double tail = mul_rn(mul_rn(mul_rn(2.0, s.hi), z), q);
+  const dd u = dd_add(dd{mul_rn(2.0, s.hi), mul_rn(2.0, s.lo)}, dd{tail, 0.0});
+  const dd lm = dd_add(GH_TAB(logc, i - 90), u);
+  const dd r = dd_add(dd_mul_d(dd{GH_LN2_HI, GH_LN2_LO}, (double)e), lm);
+  const double E = add_rn(mul_rn(fabs(s.hi), 0x1p-67), mul_rn(fabs(r.hi), 0x1p-98));
+  double y;
+  return ziv_round(r, E, &y) ? y : cr_log(x);
+}
+
+// cos x, first phase: the reduction of cr_cos (r = x - k pi/32 in double-double), then
+//   cos r = 1 - r^2/2 + z^2 (1/24 - z/720 + z^2/40320 - z^3/3628800),  z = r_hi^2,
+//   sin r = r_hi + (r_lo + r_hi ts),  ts = -z/6 + z^2/120 - ... + z^5/39916800 (double),
+// |r| <= pi/64: the leading r^2/2 in double-double, the rest in double.  Error: sin r
+// under 2^-52.6 |r_hi| z (ts to 2^-50.4 relative, times |r_hi ts| <= |r_hi| z / 6, and the
+// fma's rounding), cos r under 2^-54.5 z^2 (the double tail), the reduction, tables and
+// double-double steps under 2^-100; E = 2^-52 |r_hi| z + 2^-54 z^2 + 2^-99, so that the
+// bound shrinks with r where cos x is near zero.
+GH_HD double cr_cos_fast(double x) {
+  const double k = rint_rn(mul_rn(x, GH_32_OVER_PI));
+  dd r = dd_add(dd{x, 0.0}, dd_neg(two_prod(k, GH_PI32_1)));
+  r = dd_add(r, dd_neg(two_prod(k, GH_PI32_2)));
+  r = dd_add(r, dd{-mul_rn(k, GH_PI32_3), 0.0});
+  const int j = ((int)k) & 63;
+  const dd zz = two_prod(r.hi, r.hi);
+  const double z = zz.hi;
+  double tc = fma_rn(z, -2.755731922398589e-07, 2.48015873015873e-05);   // -1/3628800, 1/40320
+  tc = fma_rn(z, tc, -0.001388888888888889);                            // -1/720
+  tc = fma_rn(z, tc, 0.041666666666666664);                             // 1/24
+  tc = mul_rn(mul_rn(z, z), tc);
+  const double zl = fma_rn(mul_rn(2.0, r.hi), r.lo, zz.lo);                   // r^2 = z + zl to 2^-106
+  const dd cosr = dd_add(dd{1.0, 0.0}, dd_add(dd{mul_rn(-0.5, z), mul_rn(-0.5, zl)}, dd{tc, 0.0}));
+  double ts = fma_rn(z, 2.505210838544172e-08, -2.7557319223985893e-06);  // 1/39916800, -1/362880
+  ts = fma_rn(z, ts, 0.0001984126984126984);                               // 1/5040
+  ts = fma_rn(z, ts, -0.008333333333333333);                              // -1/120
+  ts = fma_rn(z, ts, 0.16666666666666666);                                // 1/6
+  ts = mul_rn(-z, ts);
+  const dd sinr = fast_two_sum(r.hi, fma_rn(r.hi, ts, r.lo));
+  const dd res = dd_add(dd_mul(GH_TAB(cos, j), cosr), dd_neg(dd_mul(GH_TAB(sin, j), sinr)));
+  double y;
+  const double E = add_rn(add_rn(mul_rn(mul_rn(fabs(r.hi), z), 0x1p-52), mul_rn(mul_rn(z, z), 0x1p-54)), 0x1p-99);
+  return ziv_round(res, E, &y) ? y : cr_cos(x);
+}
+
 // Standard normal draw keyed on k (src/core/rng.hpp:42-46 formula).
 GH_HD double gauss(uint64_t seed, uint64_t k) {
   const double u1 = uniform(seed, splitmix64(k * 2 + 1));
   const double u2 = uniform(seed, splitmix64(k * 2 + 2));
-  const double a = sqrt_rn(mul_rn(-2.0, cr_log(u1)));
-  const double c = cr_cos(mul_rn(6.283185307179586, u2));            // (2 * pi) * u2, 2*pi exact
+  const double a = sqrt_rn(mul_rn(-2.0, cr_log_fast(u1)));
+  const double c = cr_cos_fast(mul_rn(6.283185307179586, u2));       // (2 * pi) * u2, 2*pi exact
   return mul_rn(a, c);
 }
 

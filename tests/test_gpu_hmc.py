@@ -122,6 +122,30 @@ def test_reversibility(N, kind, precision, tol):
     h.close()
 
 
+def test_fp64_refresh_equals_host_draws_bit_for_bit():
+    """The FP64 refresh on the device draws every momentum with the two-phase correctly
+    rounded log and cos; the host entry point gh_rng_gauss runs the same code, so the
+    device momenta equal the host draws bit for bit (P^a = gauss(key(key(0xC3, traj),
+    s, mu, a)), pi_k = gauss(key(key(0xD4, traj), s, 2k)) + i gauss(.., 2k + 1))."""
+    import gauge_higgs_b200 as gh
+    from gauge_higgs_b200._lib import LIB
+    seed, L = 5, [4, 4, 4, 4]
+    h = gh.GaugeHiggsHMC(L, gh.FundamentalRep(3), seed=seed, precision="fp64", beta=5.7, kappa=0.1, lam=0.5)
+    h.hot(0.5)
+    h.refresh_momenta()
+    P, pi = np.asarray(h.P), np.asarray(h.pi)
+    h.close()
+    V = int(np.prod(L))
+    sp, sq = LIB.gh_rng_key(0xC3, 0, 0, 0, 0), LIB.gh_rng_key(0xD4, 0, 0, 0, 0)
+    want = np.array([[[LIB.gh_rng_gauss(seed, LIB.gh_rng_key(sp, s, mu, a, 0)) for a in range(8)] for mu in range(4)]
+                     for s in range(V)])
+    assert np.array_equal(P.reshape(V, 4, 8), want)
+    wpi = np.array([[complex(LIB.gh_rng_gauss(seed, LIB.gh_rng_key(sq, s, 2 * k, 0, 0)),
+                             LIB.gh_rng_gauss(seed, LIB.gh_rng_key(sq, s, 2 * k + 1, 0, 0))) for k in range(3)]
+                    for s in range(V)])
+    assert np.array_equal(pi.reshape(V, 3), wpi)
+
+
 def test_fp32_refresh_equals_rounded_fp64():
     """The FP32-MD refresh draws with the CUDA math library's FP64 log and cos; rounded
     to FP32 its momenta equal the FP64 mode's correctly rounded draws, bar a few."""
