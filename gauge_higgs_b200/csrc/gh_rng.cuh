@@ -21,7 +21,9 @@
 //     Taylor series in double-double on |r| <= pi/64.
 // Final rounding hi+lo gives the correctly rounded result except when the true
 // value lies within ~2^-100 relative of a rounding midpoint (probability ~2^-47
-// per call).  Host and device use the same explicitly rounded operations
+// per call).  The Gaussian calls them through a cheaper first phase (Ziv's
+// strategy, cr_log_fast / cr_cos_fast) that returns the same value whenever its
+// own error bound settles the rounding, and falls back to them otherwise.  Host and device use the same explicitly rounded operations
 // (no contraction), so both produce identical bits.
 #pragma once
 #include <stdint.h>
