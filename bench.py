@@ -501,8 +501,8 @@ def run_extra(a, dist):
                 paths = [None]
                 for path in paths:
                     h = gh.GaugeHiggsHMC([12] * 4, rep, seed=1, precision=prec, beta=5.7, kappa=0.1, lam=0.5, nmd=20)
-                    if path is None and h.rep_path() == "product" and a.c3_ab:
-                        paths.append("tensor")       # the same workload without the product path (A/B)
+                    if path is None and h.rep_path() in ("product", "pair") and a.c3_ab:
+                        paths.append("tensor")       # the same workload without the product / pair path (A/B)
                     if path is not None:
                         h.set_rep_path(path)
                     h.hot(0.8)
@@ -777,7 +777,7 @@ def main():
     ap.add_argument("--kick-tile", default="", help="fixed kick tile (e.g. 16,2,2,2) instead of the timed choice")
     ap.add_argument("--validate-traj", type=int, default=2000)
     ap.add_argument("--validate-therm", type=int, default=200)
-    ap.add_argument("--c3-ab", action="store_true", help="C3: also time product-path irreps on the tensor path")
+    ap.add_argument("--c3-ab", action="store_true", help="C3: also time product- and pair-path irreps on the tensor path")
     ap.add_argument("--c5-targets", default="2.3:0.5,2.2:0.3", help="C5: beta:lambda targets (comma list)")
     ap.add_argument("--c5-sizes", default="8,12", help="C5: lattice sizes")
     ap.add_argument("--c5-seed", type=int, default=100)

@@ -67,6 +67,8 @@ struct gh_ctx {
   // whether the link kernel goes that way (gh_set_rep_path switches it)
   ghadj::Product prod;
   bool has_prod = false;
+  // two-slot irreps (n = 2) outside the adjoint product: the register path (k_gen_pair)
+  bool has_pair = false;
   size_t gen_warp_bytes = 0, gen_px_off = 0;
   // multi-invariant potential: device copies of the channel superoperator (sparse rows)
   int* sa_ptr = nullptr;
@@ -475,6 +477,23 @@ int build_general(gh_ctx* ctx, const gh_rep_desc* r) {
     t.pq64 = d64; t.pq32 = d32; t.prow = rows; t.pK = ctx->prod.K;
     t.pnrows = (int)ctx->prod.rows.size(); t.pndiag = ctx->prod.ndiag; t.psym = ctx->prod.sym;
   }
+  t.w2_64 = nullptr; t.w2_32 = nullptr;
+  if (ctx->has_pair) {
+    const size_t nw = (size_t)r->d * r->dimT;
+    std::vector<double2> w64(nw);
+    std::vector<float2> w32(nw);
+    for (size_t i = 0; i < nw; ++i) {
+      w64[i] = make_double2(r->W[2 * i], r->W[2 * i + 1]);
+      w32[i] = make_float2((float)r->W[2 * i], (float)r->W[2 * i + 1]);
+    }
+    double2* d64;
+    float2* d32;
+    if ((rc = dalloc(ctx, &d64, nw)) || (rc = dalloc(ctx, &d32, nw))) return rc;
+    CK(cudaMemcpyAsync(d64, w64.data(), nw * sizeof(double2), cudaMemcpyHostToDevice, ctx->st));
+    CK(cudaMemcpyAsync(d32, w32.data(), nw * sizeof(float2), cudaMemcpyHostToDevice, ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));     // the host vectors go out of scope
+    t.w2_64 = d64; t.w2_32 = d32;
+  }
   t.warp_bytes = (int)ctx->gen_warp_bytes;
   t.px_off = (int)ctx->gen_px_off;
   if (ctx->use_sp) {
@@ -505,6 +524,7 @@ int gh_rep_path(const gh_ctx* ctx, int* path) {
   if (!ctx || !path) return fail(nullptr, GH_ERR_ARG, "null argument");
   *path = ctx->rep != REP_GEN ? GH_PATH_REGISTER
           : ctx->b.gen_prod    ? GH_PATH_PRODUCT
+          : ctx->b.gen_pair    ? GH_PATH_PAIR
           : (ctx->use_sp ? GH_PATH_CLOSED_FORM : GH_PATH_TENSOR);
   return GH_OK;
 }
@@ -516,8 +536,12 @@ int gh_set_rep_path(gh_ctx* ctx, int path) {
   if (path == GH_PATH_PRODUCT) {
     if (!ctx->has_prod) return fail(ctx, GH_ERR_ARG, "this irrep has no product-of-adjoints form");
     ctx->b.gen_prod = 1;
+  } else if (path == GH_PATH_PAIR) {
+    if (!ctx->has_pair) return fail(ctx, GH_ERR_ARG, "this irrep is not a two-slot irrep outside the adjoint product");
+    ctx->b.gen_pair = 1;
   } else if (path == base) {
     ctx->b.gen_prod = 0;
+    ctx->b.gen_pair = 0;
   } else {
     return fail(ctx, GH_ERR_ARG, "path not available for this context");
   }
@@ -727,6 +751,24 @@ int gh_ctx_create(int D, int N, int n_lat, const int* L, const gh_rep_desc* rep,
           for (int s0 = 0; s0 < ctx->lat_h[l].V; s0 += GP_LINKS)
             wgp.push_back(Work{l, mu, s0, std::min(GP_LINKS, ctx->lat_h[l].V - s0)});
     }
+    // two-slot irreps the product does not reach: every basis vector, as an N x N
+    // matrix, symmetric (or every one antisymmetric), which the register path needs
+    if (!ctx->has_prod && rep->W && rep->n_boxes == 2 && rep->dimT == (long)N * N) {
+      int sign = 0;
+      bool ok = true;
+      for (int b = 0; b < rep->d && ok; ++b)
+        for (int i = 0; i < N && ok; ++i)
+          for (int j = 0; j < N && ok; ++j) {
+            const double* wij = rep->W + 2 * ((size_t)b * N * N + i * N + j);
+            const double* wji = rep->W + 2 * ((size_t)b * N * N + j * N + i);
+            const double sym = std::fabs(wij[0] - wji[0]) + std::fabs(wij[1] - wji[1]);
+            const double anti = std::fabs(wij[0] + wji[0]) + std::fabs(wij[1] + wji[1]);
+            const int sg = sym < 1e-12 ? (anti < 1e-12 ? 0 : 1) : (anti < 1e-12 ? -1 : 2);
+            if (sg == 2 || (sg != 0 && sign != 0 && sg != sign)) ok = false;
+            else if (sg != 0) sign = sg;
+          }
+      ctx->has_pair = ok;
+    }
   }
   std::vector<Work> wall = wl;
   wall.insert(wall.end(), ws.begin(), ws.end());
@@ -756,7 +798,7 @@ int gh_ctx_create(int D, int N, int n_lat, const int* L, const gh_rep_desc* rep,
   }
   b.U = U; b.Us = Us; b.P = P; b.phi = phi; b.phis = phis; b.pi = pi; b.psif = psif; b.psib = psib;
   b.nw_links = (int)wl.size(); b.nw_sites = (int)ws.size(); b.nw_gen = (int)wg.size(); b.gen_warps = gw;
-  b.nw_gprod = (int)wgp.size(); b.gen_prod = ctx->has_prod ? 1 : 0;
+  b.nw_gprod = (int)wgp.size(); b.gen_prod = ctx->has_prod ? 1 : 0; b.gen_pair = ctx->has_pair ? 1 : 0;
   b.hist_cap = 1024;
   b.nlat = n_lat; b.D = D; b.N = N; b.d = ctx->d; b.rep = ctx->rep; b.scalar = ctx->scalar; b.st = ctx->st;
   if ((rc = dalloc(ctx, &b.lats, n_lat)) || (rc = dalloc(ctx, &b.w_all, wall.size())) ||

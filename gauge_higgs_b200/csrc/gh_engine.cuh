@@ -35,6 +35,7 @@ struct Bufs {
   Work* w_gprod;   // general irrep, product of adjoints: items of up to 32 links (one 32-site block)
   int nw_gprod;
   int gen_prod;    // 1: general-irrep link work through k_gen_prod (gen.pq64 set)
+  int gen_pair;    // 1: general-irrep link work through k_gen_pair (gen.w2_64 set)
   int gen_warps;   // warps per block of k_gen_links (1..GEN_WARPS, from the tensor size)
   int* blk_first;  // [nlat+1] first site item of each lattice (relative to the site items)
   Work* w_kick;    // kick items over 4-D tiles (LatDev::lt): link items then site items
@@ -110,6 +111,11 @@ struct Engine : EngineBase {
     a.work = b.w_gen; a.lats = b.lats; a.U = b.U; a.P = b.P; a.phi = b.phi; a.psif = b.psif; a.psib = b.psib;
     a.t = b.gen; a.eps = eps; a.mode = mode; a.out = out;
     a.pot = b.pot; a.sa = b.sa64; a.wpot = b.wpot;
+    if (b.gen_pair && b.gen.w2_64 && b.pot != POT_MULTI) {  // two-slot irreps in registers, one thread per link
+      a.work = b.w_all;
+      launch(k_gen_pair<D, N, R>, b.nw_links, KBLOCK, 0, b.st, a);
+      return;
+    }
     if (b.gen_prod && b.gen.pq64 && b.pot != POT_MULTI) {   // the potential's w is computed by k_gen_links
       a.work = b.w_gprod;
       if (b.gen.pK == 1) launch(k_gen_prod<D, N, R, 1>, b.nw_gprod, GP_THREADS, gen_prod_smem<N, 1, C>(b.d, b.gen.pnrows), b.st, a);

@@ -140,6 +140,8 @@ struct GenTables {                 // general irrep (src/rep/rep_general.hpp), s
   const double2* pq64; const float2* pq32;
   const int* prow;
   int pK, pnrows, pndiag, psym;
+  // two-slot irreps (n = 2): the basis W [d][N*N] dense in both precisions; null: not used
+  const double2* w2_64; const float2* w2_32;
 };
 
 template <typename R> struct V2;
@@ -999,6 +1001,99 @@ __global__ void __launch_bounds__(GP_THREADS) k_gen_prod(const GenArgs a) {
     } else {
       a.out[pi_] = (double)F;
     }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Two-slot irreps (n = 2: the symmetric and antisymmetric squares of V, e.g. the SU(3)
+// sextet {2} and antitriplet {1,1}) in registers, one thread per link.  With the irrep
+// basis W ([d][N*N], tensor index i*N + j for the slots (i, j)) the reference's tensor
+// apply (src/rep/rep_general.hpp:184-220: lift with W, U on each slot, project with W^H)
+// is, as N x N matrices,
+//   Phi = sum_b phi_b W_b,  Psi = U Phi U^T,  psi_b = sum_ij conj(W_b,ij) Psi_ij,
+// and D^dag phi the same with Psi = U^dag Phi conj(U).  Every W_b is symmetric or
+// antisymmetric, so phi_x^dag T^a_R psi_f = Tr(Phi_x^dag (T^a Psi + Psi T^aT))
+// = 2 Tr(T^a Psi Phi_x^dag), and the matter force -kappa g^a, g^a = -2 Im(phi_x^dag
+// T^a_R D phi_{x+mu}) (src/rep/representation.hpp:36-46), is 4 kappa Im Tr(T^a Psi
+// Phi_x^dag): one N x N product and the projection the fundamental uses.  Outputs and
+// modes as k_gen_links: psi_f, psi_b to the scratch fields; mode 0 P -= eps F, mode 2
+// F -> out, mode 1 psi_f only.
+// ---------------------------------------------------------------------------
+template <int N, typename C, typename R>
+__device__ __forceinline__ Mat<N, C> pair_lift(const typename V2<C>::t* Wt, int d, const R* phi, const LatDev& L, int s) {
+  Mat<N, C> M;
+  set_zero(M);
+  for (int b = 0; b < d; ++b) {
+    const cx<C> f = ldc<C>(phi, f_index(L, d, b, s));
+#pragma unroll
+    for (int t = 0; t < N * N; ++t) {
+      const typename V2<C>::t v = __ldg(Wt + b * N * N + t);
+      M.e[t] = cfma(M.e[t], f, mk<C>(v.x, v.y));
+    }
+  }
+  return M;
+}
+template <int N, typename C, typename R>
+__device__ __forceinline__ void pair_project(const typename V2<C>::t* Wt, int d, const Mat<N, C>& M, R* out,
+                                             const LatDev& L, int mu, int s) {
+  for (int b = 0; b < d; ++b) {
+    cx<C> z = zero<C>();
+#pragma unroll
+    for (int t = 0; t < N * N; ++t) {
+      const typename V2<C>::t v = __ldg(Wt + b * N * N + t);
+      z = cfma(z, mk<C>(v.x, -v.y), M.e[t]);
+    }
+    stc<C>(out, g_index(L, d, mu, b, s), z);
+  }
+}
+template <int N, typename C> __device__ __forceinline__ Mat<N, C> conj_mat(const Mat<N, C>& A) {
+  Mat<N, C> B;
+#pragma unroll
+  for (int i = 0; i < N * N; ++i) B.e[i] = conj(A.e[i]);
+  return B;
+}
+template <int D, int N, typename R>
+__global__ void __launch_bounds__(KBLOCK) k_gen_pair(const GenArgs a) {
+  pdl_enter();
+  typedef typename Cmp<R>::t C;
+  const Work w = a.work[blockIdx.x];
+  if ((int)threadIdx.x >= w.n) return;
+  const LatDev& L = a.lats[w.lat];
+  const int mu = w.mu, s = w.s0 + threadIdx.x;
+  int x[D];
+  coords<D>(L, s, x);
+  if (!below_hi<D>(L, x)) return;                      // upper halo sites of a subdomain store nothing
+  const int d = a.t.d;
+  const typename V2<C>::t* Wt = reinterpret_cast<const typename V2<C>::t*>(
+      sizeof(C) == sizeof(double) ? (const void*)a.t.w2_64 : (const void*)a.t.w2_32);
+  const R* phi = (const R*)a.phi;
+  const Mat<N, C> U = ld_link<N, C>((const R*)a.U, L, mu, s);
+  const Mat<N, C> Uc = conj_mat(U);
+  const int spm = nfwd(L, s, x[mu], mu);
+  // psi_f = D phi_{x+mu}: U Phi U^T = (U Phi) conj(U)^dag
+  const Mat<N, C> Psi = mm_nd(mm(U, pair_lift<N, C>(Wt, d, phi, L, spm)), Uc);
+  pair_project<N, C>(Wt, d, Psi, (R*)a.psif, L, mu, s);
+  if (a.mode == 1) return;
+  const Mat<N, C> Phx = pair_lift<N, C>(Wt, d, phi, L, s);
+  // psi_b = D^dag phi_x: U^dag Phi conj(U)
+  pair_project<N, C>(Wt, d, mm(mm_dn(U, Phx), Uc), (R*)a.psib, L, mu, s);
+  if (!in_box<D>(L, x)) return;                        // momentum updates: interior links only
+  Mat<N, C> M = mm_nd(Psi, Phx);
+  const C k4 = C(4) * (C)L.kappa;
+#pragma unroll
+  for (int i = 0; i < N * N; ++i) M.e[i] = scale(M.e[i], k4);
+  constexpr int ng = N * N - 1;
+  C F[ng];
+  im_tr_proj<N, C>(M, F);
+  const long long pb = p_index(L, ng, mu, 0, s);
+  if (a.mode == 0) {
+    R* P = (R*)a.P;
+    const C eps = (C)a.eps;
+#pragma unroll
+    for (int g = 0; g < ng; ++g) P[pb + g * ULANE] = (R)((C)P[pb + g * ULANE] - eps * F[g]);
+  } else {
+#pragma unroll
+    for (int g = 0; g < ng; ++g) a.out[pb + g * ULANE] = (double)F[g];
   }
 }
 

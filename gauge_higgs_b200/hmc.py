@@ -513,18 +513,19 @@ class Ensemble:
                  acc.ctypes.data_as(C.POINTER(C.c_uint64)), _dptr(kap))
         return att, acc, kap
 
-    _PATHS = {0: "register", 1: "tensor", 2: "closed_form", 3: "product"}
+    _PATHS = {0: "register", 1: "tensor", 2: "closed_form", 3: "product", 4: "pair"}
 
     def rep_path(self):
         """How the device applies D(U): "register" (fundamental, adjoint), "tensor"
-        (general irreps), "closed_form" (large single-row irreps) or "product" (irreps
-        inside the adjoint's one- or two-fold product, e.g. the SU(3) octet and 27-plet)."""
+        (general irreps), "closed_form" (large single-row irreps), "product" (irreps
+        inside the adjoint's one- or two-fold product, e.g. the SU(3) octet and 27-plet)
+        or "pair" (two-slot irreps outside it, e.g. the SU(3) sextet and antitriplet)."""
         p = C.c_int()
         self.ctx("gh_rep_path", C.byref(p))
         return self._PATHS[p.value]
 
     def set_rep_path(self, path):
-        """Switch a general irrep between "product" and the path it takes without it."""
+        """Switch a general irrep between "product" or "pair" and the path it takes without them."""
         code = {v: k for k, v in self._PATHS.items()}[path]
         self.ctx("gh_set_rep_path", code)
 

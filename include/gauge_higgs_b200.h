@@ -53,7 +53,7 @@ enum { GH_REP_NONE = 0, GH_REP_FUND = 1, GH_REP_ADJ = 2, GH_REP_GENERAL = 3 };
 enum { GH_PREC_FP64 = 0, GH_PREC_FP32_MD = 1, GH_PREC_FP32_ALL = 2 };
 enum { GH_LEAPFROG = 0, GH_OMELYAN = 1 };
 /* How D(U) of the scalar's representation is applied on the device (gh_rep_path). */
-enum { GH_PATH_REGISTER = 0, GH_PATH_TENSOR = 1, GH_PATH_CLOSED_FORM = 2, GH_PATH_PRODUCT = 3 };
+enum { GH_PATH_REGISTER = 0, GH_PATH_TENSOR = 1, GH_PATH_CLOSED_FORM = 2, GH_PATH_PRODUCT = 3, GH_PATH_PAIR = 4 };
 
 /* Representation R of the scalar.  Replaces the Representation<N> object
  * (src/rep/representation.hpp:12-32).  GENERAL carries the host-built tables of
@@ -350,9 +350,12 @@ int gh_rep_product_matrix(int N, const gh_rep_desc* rep, const double* U, double
  * applied K times, a projection -- the reference's tensor matrix to rounding.  The
  * multi-invariant potential's per-site term is computed on the tensor / closed-form
  * path, so contexts with that potential use it for their link work.
+ * Two-slot irreps outside that product (n = 2: SU(3) sextet {2}, antitriplet {1,1})
+ * take GH_PATH_PAIR: one thread per link, phi lifted by W to an N x N matrix Phi,
+ * D(U) phi the projection of U Phi U^T, the matter force from U Phi_y U^T Phi_x^dag.
  * gh_rep_path: the path a context uses.
- * gh_set_rep_path: switch between GH_PATH_PRODUCT (when available) and the path the
- *   context would use without it; GH_ERR_ARG for any other path.
+ * gh_set_rep_path: switch between GH_PATH_PRODUCT or GH_PATH_PAIR (when available) and
+ *   the path the context would use without them; GH_ERR_ARG for any other path.
  * gh_sympow_matrix: host-only evaluation of the closed form D(U) (U: N x N complex
  *   row-major; D: d x d complex) and the number of terms; GH_ERR_REP when the
  *   irrep has no closed form (message through gh_last_error(NULL)). */

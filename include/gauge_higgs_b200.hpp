@@ -154,8 +154,9 @@ class GaugeHiggsHMC {
 
   gh_ctx* context() { sync_params(); return ctx_; }
   const Representation& rep() const { return rep_; }
-  // how the device applies D(U): GH_PATH_REGISTER / GH_PATH_TENSOR / GH_PATH_CLOSED_FORM
-  // (the closed form stands in for the reference's GeneralRep::use_fast path)
+  // how the device applies D(U): GH_PATH_REGISTER / GH_PATH_TENSOR / GH_PATH_CLOSED_FORM /
+  // GH_PATH_PRODUCT / GH_PATH_PAIR (the closed form stands in for the reference's
+  // GeneralRep::use_fast path; product and pair are exact re-expressions of the tensor apply)
   int rep_path() const { int p = 0; check(gh_rep_path(ctx_, &p), ctx_); return p; }
 
   // initial fields (src/core/fields.hpp:25-34, src/core/scalar_field.hpp:34-50)

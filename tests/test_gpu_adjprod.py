@@ -18,7 +18,7 @@ def rel_err(a, b):
 
 
 @pytest.mark.parametrize("N,rows,real,path", [(3, [2, 1], True, "product"), (3, [4, 2], True, "product"),
-                                              (3, [3, 3], False, "product"), (3, [2], False, "tensor"),
+                                              (3, [3, 3], False, "product"), (3, [2], False, "pair"),
                                               (2, [4], False, "product"), (2, [12], False, "closed_form")])
 def test_path_selection(N, rows, real, path):
     import gauge_higgs_b200 as gh

@@ -55,7 +55,8 @@ def _whole(G, rep, N, precision, seed, beta, kappa, lam, nmd, integ):
 
 CASES = [("fund3", [4, 4, 4, 6], [1, 1, 1, 2], "fp64"), ("fund3", [4, 4, 4, 6], [1, 1, 2, 2], "fp64"),
          ("fund3", [4, 4, 4, 6], [1, 1, 2, 2], "fp32"), ("none2", [4, 4, 6, 4], [1, 2, 3, 1], "fp64"),
-         ("adj2", [4, 4, 4, 4], [2, 1, 1, 2], "fp64"), ("27plet", [2, 2, 3, 4], [1, 1, 1, 2], "fp64")]
+         ("adj2", [4, 4, 4, 4], [2, 1, 1, 2], "fp64"), ("27plet", [2, 2, 3, 4], [1, 1, 1, 2], "fp64"),
+         ("sextet", [2, 2, 3, 4], [1, 1, 1, 2], "fp64")]
 
 
 @pytest.mark.parametrize("kind,G,P,precision", CASES)
@@ -64,7 +65,7 @@ def test_decomposed_run_equals_whole_lattice(kind, G, P, precision):
     from gauge_higgs_b200.domain import DomainHMC, InProcessTransport
     N = 2 if kind.endswith("2") else 3
     rep = {"fund3": gh.FundamentalRep(3), "none2": None, "adj2": gh.AdjointRep(2),
-           "27plet": gh.GeneralRep(3, [4, 2], real=True)}[kind]
+           "27plet": gh.GeneralRep(3, [4, 2], real=True), "sextet": gh.GeneralRep(3, [2])}[kind]
     beta, kappa, lam, nmd = (5.7, 0.1, 0.5, 6) if N == 3 else (2.3, 0.2, 0.5, 8)
     whole = _whole(G, rep, N, precision, 7, beta, kappa, lam, nmd, "omelyan")
     tr = InProcessTransport(G, P)

@@ -17,7 +17,7 @@ def test_path_selection():
     import gauge_higgs_b200 as gh
     cases = [(gh.FundamentalRep(2), "register"), (gh.GeneralRep(2, [12]), "closed_form"),
              (gh.GeneralRep(2, [17]), "closed_form"), (gh.GeneralRep(3, [8]), "closed_form"),
-             (gh.GeneralRep(3, [2]), "tensor"), (gh.GeneralRep(3, [2, 1]), "product")]
+             (gh.GeneralRep(3, [2]), "pair"), (gh.GeneralRep(3, [2, 1]), "product")]
     for rep, path in cases:
         h = gh.GaugeHiggsHMC([2, 2, 2], rep, seed=1)
         assert h.rep_path() == path, (rep.name(), h.rep_path())
