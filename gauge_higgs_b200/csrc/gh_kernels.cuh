@@ -1175,12 +1175,10 @@ __global__ void __launch_bounds__(KBLOCK) k_drift(const DriftArgs a) {
     const R* P = (const R*)a.P;
     A v[ng];
     const long long pb = p_index(L, ng, mu, 0, s);
+    const A eps = (A)a.eps;
 #pragma unroll
-    for (int g = 0; g < ng; ++g) v[g] = (A)P[pb + g * ULANE];
-    Mat<N, A> H = alg_to_mat<N, A>(v);
-#pragma unroll
-    for (int i = 0; i < N * N; ++i) H.e[i] = scale(H.e[i], (A)a.eps);
-    const Mat<N, A> E = expi<N>(H);
+    for (int g = 0; g < ng; ++g) v[g] = (A)P[pb + g * ULANE] * eps;   // eps P in algebra coefficients
+    const Mat<N, A> E = expi<N>(alg_to_mat<N, A>(v));
     const Mat<N, A> Uo = ld_link_rw<N, A>((const R*)a.U, L, mu, s);
     Mat<N, A> Un;
     if constexpr (PROJ) {

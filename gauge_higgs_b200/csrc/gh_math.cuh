@@ -372,31 +372,46 @@ template <typename T> GH_HD Mat<3, T> herm_sq3(const Mat<3, T>& Q) {
   }
   return R;
 }
+// det of a Hermitian 3x3 (real diagonal d_i, upper entries a = q01, b = q02, c = q12):
+//   d0 d1 d2 + 2 Re(a c conj(b)) - d0 |c|^2 - d1 |b|^2 - d2 |a|^2
+template <typename T> GH_HD T det_herm3(const Mat<3, T>& Q) {
+  const T d0 = Q.e[0].re, d1 = Q.e[4].re, d2 = Q.e[8].re;
+  const cx<T> a = Q.e[1], b = Q.e[2], c = Q.e[5];
+  const cx<T> ac = mul(a, c);
+  T r = d0 * d1 * d2;
+  r = fmad(T(2), fmad(ac.re, b.re, ac.im * b.im), r);
+  r = fmad(-d0, norm2(c), r);
+  r = fmad(-d1, norm2(b), r);
+  r = fmad(-d2, norm2(a), r);
+  return r;
+}
 template <typename T> GH_HD Mat<3, T> expi3(const Mat<3, T>& H) {
   T nrm2 = fnorm2(H);               // scale until ||H||_F / 2^s <= 1/2, compared squared
   int s = 0;
   while (nrm2 > T(0.25) && s < 64) { nrm2 *= T(0.25); ++s; }   // bounded: a non-finite H ends as NaN
-  const T sc = (T)ldexp(1.0, -s);
-  Mat<3, T> Q;
+  Mat<3, T> Q = H;
+  if (s > 0) {                      // rare: the MD step keeps ||eps P|| well below 1/2
+    const T sc = (T)ldexp(1.0, -s);
 #pragma unroll
-  for (int i = 0; i < 9; ++i) Q.e[i] = scale(H.e[i], sc);
+    for (int i = 0; i < 9; ++i) Q.e[i] = scale(H.e[i], sc);
+  }
   const Mat<3, T> Q2 = herm_sq3(Q);   // H (and Q) Hermitian: built from real algebra coefficients
   const T c1 = T(0.5) * (Q2.e[0].re + Q2.e[4].re + Q2.e[8].re);
-  const T c0 = det<3, T>(Q).re;
-  T a = 1, b = 0, g = 0, coef = 1;
+  const T c0 = det_herm3(Q);
+  // (a, b, g): the coefficients of Q^n / n! in (I, Q, Q^2), advanced two terms per trip
+  // (i^n = i, -1 for n = 4k+1, 4k+2 and -i, 1 for n = 4k+3, 4k+4)
+  T a = 1, b = 0, g = 0;
   T f0r = 1, f0i = 0, f1r = 0, f1i = 0, f2r = 0, f2i = 0;
-  for (int n = 1; n <= 40; ++n) {
-    const T an = c0 * g, bn = a + c1 * g, gn = b;
-    a = an; b = bn; g = gn;
-    coef *= (T)inv_int(n);
-    const T ta = coef * a, tb = coef * b, tg = coef * g;
-    switch (n & 3) {   // i^n = 1, i, -1, -i
-      case 0: f0r += ta; f1r += tb; f2r += tg; break;
-      case 1: f0i += ta; f1i += tb; f2i += tg; break;
-      case 2: f0r -= ta; f1r -= tb; f2r -= tg; break;
-      default: f0i -= ta; f1i -= tb; f2i -= tg; break;
-    }
-    if (fabs(ta) + fabs(tb) + fabs(tg) < T(ExpTol<T>::v)) break;
+#pragma unroll
+  for (int n = 1; n < 40; n += 2) {
+    const T sg = (n & 2) ? T(-1) : T(1);
+    T r = (T)inv_int(n);
+    T an = c0 * g * r, bn = fmad(c1, g, a) * r, gn = b * r;
+    f0i = fmad(sg, an, f0i); f1i = fmad(sg, bn, f1i); f2i = fmad(sg, gn, f2i);
+    r = (T)inv_int(n + 1);
+    a = c0 * gn * r; b = fmad(c1, gn, an) * r; g = bn * r;
+    f0r = fmad(-sg, a, f0r); f1r = fmad(-sg, b, f1r); f2r = fmad(-sg, g, f2r);
+    if (fabs(a) + fabs(b) + fabs(g) < T(ExpTol<T>::v)) break;
   }
   Mat<3, T> E;
 #pragma unroll
