@@ -511,23 +511,30 @@ __device__ __forceinline__ void kick_link_dispatch(const KickArgs& a, const LatD
   }
 }
 
-// Occupancy: resident kick blocks per SM.  FP32: 5 (96 registers, a few spilled);
-// FP64: 3 (168 registers).  Measured in the trajectory at SU(3) 16^4 these beat 4 / 2
-// by ~4%: the extra warps hide more of the L2 latency than the spills cost; 6 (80
-// registers) spills too much.
+// Occupancy: resident kick blocks per SM.  FP32 fundamental: 7 (72 registers, 40 bytes
+// spilled); other FP32 kicks: 5 (the adjoint's commutator terms spill 432 bytes at 72
+// registers against 28 at 96); FP64: 3 (168 registers).  Measured at SU(3) 16^4
+// (fundamental): FP32 5 and 7 blocks run the kick alone at the same 24.5 us and 7 makes
+// the trajectory 1.4% faster, 6 (80 registers) 2.5% slower; 4 / 2 lose ~4% to 5 / 3
+// (fewer warps to hide the L2 latency).
 #ifndef GH_KICK_MINB_F32
 #define GH_KICK_MINB_F32 5
+#endif
+#ifndef GH_KICK_MINB_F32_FUND
+#define GH_KICK_MINB_F32_FUND 7
 #endif
 #ifndef GH_KICK_MINB_F64
 #define GH_KICK_MINB_F64 3
 #endif
-template <typename R> struct KickMinBlocks { static constexpr int v = GH_KICK_MINB_F32 * 128 / KICK_BLOCK; };
-template <> struct KickMinBlocks<double> {
+template <typename R, int REP> struct KickMinBlocks {
+  static constexpr int v = (REP == REP_FUND ? GH_KICK_MINB_F32_FUND : GH_KICK_MINB_F32) * 128 / KICK_BLOCK;
+};
+template <int REP> struct KickMinBlocks<double, REP> {
   static constexpr int v = GH_KICK_MINB_F64 * 128 / KICK_BLOCK > 0 ? GH_KICK_MINB_F64 * 128 / KICK_BLOCK : 1;
 };
 
 template <int D, int N, typename R, int REP>
-__global__ void __launch_bounds__(KICK_BLOCK, KickMinBlocks<R>::v) k_kick(const KickArgs a) {
+__global__ void __launch_bounds__(KICK_BLOCK, KickMinBlocks<R, REP>::v) k_kick(const KickArgs a) {
   pdl_enter();
   const Work w = a.work[blockIdx.x];
   const LatDev& L = a.lats[w.lat];
