@@ -171,6 +171,12 @@ class ClockSampler:
                 "source": "nvidia-smi"}
 
 
+def gbps(nbytes, ms):
+    """Bytes over a launch time in ms as GB/s; None when the time is not positive (a
+    difference of two timings can be, e.g. under a profiler that serialises launches)."""
+    return round(nbytes / (ms / 1e3) / 1e9, 1) if ms > 0 else None
+
+
 def launches_per_traj(nmd, prec):
     # refresh 1 + (measure + finalize) x 2 + kicks (2 nmd + 1) + drifts 2 nmd
     # + end-of-trajectory reunitarisation (FP64 mode only) + Metropolis 1 + restore 1
@@ -329,9 +335,9 @@ def run_ours(a, dist):
                                   "(drift = pair - kick), fields L2-resident as inside a trajectory"),
                 "share_of_trajectory": round((share_kick if dom == "kick" else share_drift) / (r["ms"] / K), 3),
                 "fp64": {"kick_ms": round(res["fp64"]["kick_ms"], 5), "drift_ms": round(res["fp64"]["drift_ms"], 5),
-                         "kick_GBps": round(V * ALG_BYTES["kick"]["fp64"] / (res["fp64"]["kick_ms"] / 1e3) / 1e9, 1)},
+                         "kick_GBps": gbps(V * ALG_BYTES["kick"]["fp64"], res["fp64"]["kick_ms"])},
                 "fp32": {"kick_ms": round(r["kick_ms"], 5), "drift_ms": round(r["drift_ms"], 5),
-                         "drift_GBps": round(V * ALG_BYTES["drift"]["fp32"] / (r["drift_ms"] / 1e3) / 1e9, 1)},
+                         "drift_GBps": gbps(V * ALG_BYTES["drift"]["fp32"], r["drift_ms"])},
                 "fp32_all": {"kick_ms": round(res["fp32-all"]["kick_ms"], 5),
                              "drift_ms": round(res["fp32-all"]["drift_ms"], 5)},
                 "compute": compute}

@@ -513,10 +513,12 @@ __device__ __forceinline__ void kick_link_dispatch(const KickArgs& a, const LatD
 
 // Occupancy: resident kick blocks per SM.  FP32 fundamental: 7 (72 registers, 40 bytes
 // spilled); other FP32 kicks: 5 (the adjoint's commutator terms spill 432 bytes at 72
-// registers against 28 at 96); FP64: 3 (168 registers).  Measured at SU(3) 16^4
-// (fundamental): FP32 5 and 7 blocks run the kick alone at the same 24.5 us and 7 makes
-// the trajectory 1.4% faster, 6 (80 registers) 2.5% slower; 4 / 2 lose ~4% to 5 / 3
-// (fewer warps to hide the L2 latency).
+// registers against 28 at 96); FP64 fundamental: 4 (128 registers, 64 bytes spilled),
+// other FP64 kicks 3 (the adjoint spills 1.3 KB at 128 registers).  Measured at
+// SU(3) 16^4 (fundamental): the kick alone runs the same at FP32 5 and 7 blocks (24.5
+// us) and at FP64 3 and 4 (40.7 / 40.9 us), while the trajectory with the higher
+// occupancy is 1.4% (FP32) and 1.7% (FP64) faster -- the next launch's blocks find room
+// sooner; FP32 6 blocks (80 registers) was 2.5% slower; FP32 4 / FP64 2 lose ~4%.
 #ifndef GH_KICK_MINB_F32
 #define GH_KICK_MINB_F32 5
 #endif
@@ -526,11 +528,15 @@ __device__ __forceinline__ void kick_link_dispatch(const KickArgs& a, const LatD
 #ifndef GH_KICK_MINB_F64
 #define GH_KICK_MINB_F64 3
 #endif
+#ifndef GH_KICK_MINB_F64_FUND
+#define GH_KICK_MINB_F64_FUND 4
+#endif
 template <typename R, int REP> struct KickMinBlocks {
   static constexpr int v = (REP == REP_FUND ? GH_KICK_MINB_F32_FUND : GH_KICK_MINB_F32) * 128 / KICK_BLOCK;
 };
 template <int REP> struct KickMinBlocks<double, REP> {
-  static constexpr int v = GH_KICK_MINB_F64 * 128 / KICK_BLOCK > 0 ? GH_KICK_MINB_F64 * 128 / KICK_BLOCK : 1;
+  static constexpr int b = REP == REP_FUND ? GH_KICK_MINB_F64_FUND : GH_KICK_MINB_F64;
+  static constexpr int v = b * 128 / KICK_BLOCK > 0 ? b * 128 / KICK_BLOCK : 1;
 };
 
 template <int D, int N, typename R, int REP>
