@@ -459,7 +459,7 @@ def run_extra(a, dist):
     from oracle.oracle import Reference, RefSession, have_reference, LEAPFROG, OMELYAN
     stream = torch.cuda.Stream()
     torch.cuda.set_stream(stream)
-    ref = Reference() if have_reference() else None
+    ref = Reference() if (have_reference() and not a.no_cpu) else None
     cores = ref.set_threads(os.cpu_count() or 1) if ref else 0
 
     def gpu_rate(h, K, W=3):
@@ -717,16 +717,18 @@ def run_extra(a, dist):
             h.hot(0.8)
             h.phi_gaussian(12345, 0.3)
             h.autotune(reps=2)
+            h.refresh_momenta()       # Gaussian momenta: the drift's exponential does its real work
             V = 32 ** 4
             res = {}
             for which in ("kick", "drift"):
-                fn = h.kick if which == "kick" else h.drift
-                fn(0.0)
+                # the kick with eps 0 leaves P as drawn; the drift takes the Omelyan half step 1/32
+                fn, eps = (h.kick, 0.0) if which == "kick" else (h.drift, 1.0 / 32)
+                fn(eps)
                 torch.cuda.synchronize()
                 e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
                 e0.record(stream)
                 for _ in range(10):
-                    fn(0.0)
+                    fn(eps)
                 e1.record(stream)
                 torch.cuda.synchronize()
                 ms = e0.elapsed_time(e1) / 10
