@@ -451,7 +451,7 @@ def run_reference(a, dist):
 
 
 def run_extra(a, dist):
-    """Additional measurements (not the headline line): the other configurations of the benchmark set
+    """Additional measurements (not the headline line): the other workloads of the benchmark
     and a lattice larger than L2.  One JSON line per case, rank 0, one GPU."""
     import torch
     torch.cuda.set_device(dist.local)

@@ -1,10 +1,10 @@
-"""The learned coupling-scan campaign of the benchmark set's configuration 5.
+"""The learned coupling-scan campaign: locate kappa_c of SU(2) + fundamental Higgs with an MLP surrogate.
 
 An ensemble of five MLPs 4 -> 128 -> 128 -> 128 -> 3 (SiLU, FP32 weights, BF16
 activations; gauge_higgs_b200.mlp, trained by the library's own CUDA kernels with Adam
 at lr 1e-3) maps (beta, kappa, lambda, 1/L) over beta in [2.1, 2.5], kappa in
 [0.15, 0.35], lambda in [0.1, 1.0] to (<L_link>, log chi_link, plaquette) of the SU(2)
-fundamental-Higgs model.  It is trained first on the batch of configuration 4 (64
+fundamental-Higgs model.  It is trained first on the 64-lattice tempering batch (64
 lattices, 16 kappas in 0.22..0.31 for each L in 6, 8, 10, 12, at beta 2.3, lambda 0.5)
 and on 12 kappas evenly over the kappa domain at every target's (beta, lambda) and size,
 all short runs; then each
@@ -103,7 +103,7 @@ class Surrogate4D:
 
 
 def c4_points():
-    """Configuration 4's batch: 16 kappas 0.22..0.31 for each L in 6, 8, 10, 12 (beta 2.3, lambda 0.5)."""
+    """The 64-lattice tempering batch: 16 kappas 0.22..0.31 for each L in 6, 8, 10, 12 (beta 2.3, lambda 0.5)."""
     return [(2.3, 0.22 + 0.006 * i, 0.5, L) for L in (6, 8, 10, 12) for i in range(16)]
 
 

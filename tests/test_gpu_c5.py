@@ -1,6 +1,6 @@
-"""The learned coupling-scan campaign on the benchmark set's configuration 5
+"""The learned coupling-scan campaign (SU(2) + fundamental Higgs, kappa_c from an MLP surrogate)
 (gauge_higgs_b200/c5.py): an ensemble of five 4-128-128-128-3 MLPs over (beta, kappa,
-lambda, 1/L), trained by the library's own kernels on configuration 4's batch and 12
+lambda, 1/L), trained by the library's own kernels on the 64-lattice tempering batch and 12
 kappas over the kappa domain at every target and size, then one active-learning round of 32 points near
 the predicted chi_link peaks, each checked by 1000-trajectory plain HMC at 8^4 and
 12^4.  Targets: kappa_c at two (beta, lambda) points, each at L = 8 and 12.

@@ -1,5 +1,5 @@
 """Statistical parity with the reference on the SU(2) + fundamental Higgs 6^4
-configuration as the benchmark set states it: beta 2.3, kappa 0.20, lambda 0.5,
+workload as specified: beta 2.3, kappa 0.20, lambda 0.5,
 leapfrog nmd 20, tau 1, hot start (sigma 0.8) from Rng seed 1, scalar field
 Gaussian (sigma 0.3, stream 12345); 50 thermalisation then 1000 measured
 trajectories on each side.
