@@ -158,6 +158,9 @@ class GaugeHiggsHMC {
   // GH_PATH_PRODUCT / GH_PATH_PAIR (the closed form stands in for the reference's
   // GeneralRep::use_fast path; product and pair are exact re-expressions of the tensor apply)
   int rep_path() const { int p = 0; check(gh_rep_path(ctx_, &p), ctx_); return p; }
+  // switch a general irrep between GH_PATH_PRODUCT / GH_PATH_PAIR and the path it takes
+  // without them (an A/B of the same workload); throws for a path the irrep does not have
+  void set_rep_path(int path) { check(gh_set_rep_path(ctx_, path), ctx_); }
 
   // initial fields (src/core/fields.hpp:25-34, src/core/scalar_field.hpp:34-50)
   void hot(double sigma = 1.0) { check(gh_hot_start(ctx_, sigma), ctx_); }
