@@ -8,7 +8,6 @@ The kernels use these functions unchanged, so the checks pin the device arithmet
 import os
 import subprocess
 
-import numpy as np
 import pytest
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))

@@ -8,8 +8,6 @@ small).  The GPU kernels compile the same functions."""
 import os
 import subprocess
 
-import pytest
-
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 SRC = r'''
